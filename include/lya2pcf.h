@@ -1,0 +1,127 @@
+/*
+ * lya2pcf B200 pair-binning library: C ABI.
+ *
+ * One context per thread of control; every call returns an int status
+ * (LYA_OK == 0) and never throws or exits; lya_last_error() describes the most
+ * recent failure.  Host buffers are caller-owned and only read or written
+ * during the call; the library owns all device memory of a context and runs
+ * every kernel on the context's own stream.
+ *
+ * Each entry point names the reference routine whose role it takes
+ * (lya2pcf, file:line).
+ */
+#ifndef LYA2PCF_H
+#define LYA2PCF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LYA_OK 0
+#define LYA_ERR_ARG 1      /* bad argument: null pointer, size, shape, option */
+#define LYA_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define LYA_ERR_ALLOC 3    /* device or host allocation failed */
+#define LYA_ERR_STATE 4    /* call out of order (e.g. run before upload) */
+#define LYA_ERR_DATA 5     /* input data violates a documented requirement */
+#define LYA_ERR_GUARD 6    /* guard band narrower than the FP32 error bound */
+#define LYA_ERR_DEVICE 7   /* a kernel reported an internal error flag */
+
+/* kernels of lya_corr_run */
+#define LYA_KERNEL_FP32_GUARDED 0 /* FP32 diagonal-run kernel, FP64 recheck in the guard band */
+#define LYA_KERNEL_FP64_DIAGONAL 1 /* same walk, FP64 geometry and run sums */
+#define LYA_KERNEL_FP64_PLAIN 2    /* every pixel pair, FP64, one shared atomic per quantity */
+
+/* histogram quantities, in output order: sum w1w2, sum dw1dw2, sum w1w2*rp,
+ * sum w1w2*rt, sum w1w2*(z1+z2)/2 */
+#define LYA_NQ 5
+
+typedef struct lya_ctx lya_ctx;
+
+typedef struct {
+  int32_t kernel;          /* LYA_KERNEL_* */
+  double guard;            /* guard half-width around bin edges, Mpc/h (FP32 kernel) */
+  int32_t warps_per_block; /* 0 = autotuned/default */
+  int32_t blocks_per_sm;   /* 0 = default (1) */
+  int32_t use_graph;       /* replay the run through a captured CUDA graph */
+} lya_corr_opts;
+
+typedef struct {
+  double ref_pairs;        /* sum over forest pairs of len1*len2 (reference pair count) */
+  double evaluated_pairs;  /* pixel pairs the kernel evaluated */
+  double guard_rechecks;   /* pairs re-evaluated in FP64 inside the guard band */
+  double runs_flushed;     /* register runs flushed into the shared histogram */
+  double in_range_pairs;   /* pairs that landed in a bin */
+  double kernel_ms;        /* device time of the last lya_corr_run pair kernel */
+  double build_ms;         /* device time of the last lya_build_pairs */
+  int64_t n_pairs;         /* forest pairs in the work queue */
+  int32_t n_slots;
+  int32_t n_forests;
+  double guard_bound;      /* proven FP32 error bound, Mpc/h */
+} lya_stats_t;
+
+/* ----------------------------------------------------------------- context */
+int lya_ctx_create(int device, lya_ctx** out);
+int lya_ctx_destroy(lya_ctx* ctx);
+/* Message of the last failure on ctx (or of the last failure of this thread
+ * when ctx is NULL). Never NULL. */
+const char* lya_last_error(const lya_ctx* ctx);
+int lya_version(void);
+
+/* Histogram geometry; replaces the module constants rpmax, rtmax, numpix_rp,
+ * numpix_rt (parameters.py:18-23) read by pair_correlation
+ * (cuda_kernels.cpp:94-99).  np*nt <= 4096. */
+int lya_set_bins(lya_ctx* ctx, double rpmax, double rtmax, int32_t np, int32_t nt);
+
+/* Forest catalogue upload; replaces correlation_procedures_pycuda.init
+ * (correlation_procedures_pycuda.py:16-111), which packs padded FP64 arrays and
+ * copies them to the device.  Forests are given in forest.index order as CSR:
+ * forest f owns pixels start[f]..start[f+1]-1 of dc, w, dw, z (and dl).
+ * owner_slot[f] is the output histogram of pairs whose first forest is f (the
+ * healpix pixel of forest_class.py:22-25, renumbered 0..n_slots-1) and must be
+ * non-decreasing in f.  name[] identifies the quasar (same name: no pair).
+ * dl, omega, odl2 may be NULL (needed by the distortion only). */
+int lya_upload_forests(lya_ctx* ctx, int64_t n_forests, const int64_t* start, const double* dc, const double* w,
+                       const double* dw, const double* z, const double* dl, const double* ux, const double* uy,
+                       const double* uz, const double* ra, const double* dec, const int64_t* name,
+                       const int32_t* owner_slot, int32_t n_slots, const double* omega, const double* odl2);
+
+/* Neighbour lists on the device; replaces quasar.neighborhood
+ * (forest_class.py:78-98) called per forest by two_point_per_pixel
+ * (correlation_procedures_pycuda.py:144): f2 is a neighbour of f1 when
+ * ((x1*x2 + y1*y2) + z1*z2) > mumin (mumin = cos(angmax) as numpy computes it),
+ * name1 != name2 and ra1 < ra2.  The work queue holds every (f1, f2) pair,
+ * grouped by f1.  *n_pairs_out receives the number of forest pairs. */
+int lya_build_pairs(lya_ctx* ctx, double angmax, double mumin, int64_t* n_pairs_out);
+
+/* Explicit work queue from the host, in place of lya_build_pairs: forest
+ * pairs (f1[k], f2[k]) grouped by f1 (f1 non-decreasing). */
+int lya_set_pairs(lya_ctx* ctx, int64_t n_pairs, const int32_t* f1, const int32_t* f2);
+
+/* Copy the current work queue to the host (n_pairs entries each). */
+int lya_get_pairs(lya_ctx* ctx, int32_t* f1, int32_t* f2);
+
+/* Per-slot pair histograms of the whole work queue in one persistent launch;
+ * replaces the per-forest launch loop of two_point_per_pixel
+ * (correlation_procedures_pycuda.py:141-166) and the pair_correlation kernel
+ * (cuda_kernels.cpp:90-162).  Results stay on the device until lya_corr_get. */
+int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts);
+
+/* Copy slots [slot_first, slot_first+n) to the host: hist[n][LYA_NQ][np*nt]
+ * (FP64) and counts[n][np*nt] (pair counts).  Either pointer may be NULL. */
+int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double* hist, uint64_t* counts);
+
+/* Gradient of L = sum_b g[b] * DW_b / W_b (totals over all slots of the last
+ * lya_corr_run) with the pair bins held fixed: grad_dw and grad_w per pixel of
+ * the catalogue (CSR order).  No reference counterpart. */
+int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w);
+
+int lya_stats(lya_ctx* ctx, lya_stats_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LYA2PCF_H */

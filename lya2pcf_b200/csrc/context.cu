@@ -1,0 +1,349 @@
+// Context, catalogue upload and result copy-out of the lya2pcf B200 library.
+//
+// The upload replaces correlation_procedures_pycuda.init
+// (correlation_procedures_pycuda.py:16-111): instead of host-packed
+// [n_forest x max_lenght] padded FP64 arrays, the caller's unpadded CSR arrays
+// are copied once and packed on the device into
+//   * FP64 per-pixel arrays (dc, w, dw, z, dl) on a 4-pixel-aligned CSR, read by
+//     the FP64 kernels and by the FP32 kernel's guard-band recheck;
+//   * an FP32 float4 per pixel (dc_hi, dc_lo, w, dw) plus FP32 z, read by the
+//     FP32 kernel: dc = dc_hi + dc_lo to ~2^-48 relative, so FP32 differences
+//     of comoving distances stay accurate to ~1e-5 Mpc/h.
+#include <algorithm>
+#include <cstring>
+
+#include "lya_internal.cuh"
+
+static thread_local std::string g_thread_err;
+
+int lya_fail(lya_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_thread_err = buf;
+  if (ctx) ctx->err = buf;
+  return code;
+}
+
+void lya_free_catalog(DevCatalog& c) {
+  lya_free(c.pstart); lya_free(c.len); lya_free(c.sorted); lya_free(c.slot);
+  lya_free(c.ux); lya_free(c.uy); lya_free(c.uz); lya_free(c.ra); lya_free(c.dec); lya_free(c.name);
+  lya_free(c.omega); lya_free(c.odl2);
+  lya_free(c.dc); lya_free(c.w); lya_free(c.dw); lya_free(c.z); lya_free(c.dl);
+  lya_free(c.pix4); lya_free(c.z32); lya_free(c.pix8);
+  c = DevCatalog{};
+}
+
+void lya_free_queue(WorkQueue& q) {
+  lya_free(q.f1); lya_free(q.f2);
+  q = WorkQueue{};
+}
+
+extern "C" int lya_version(void) { return 10000; }
+
+extern "C" const char* lya_last_error(const lya_ctx* ctx) {
+  if (ctx) return ctx->err.c_str();
+  return g_thread_err.c_str();
+}
+
+extern "C" int lya_ctx_create(int device, lya_ctx** out) {
+  if (!out) return lya_fail(nullptr, LYA_ERR_ARG, "lya_ctx_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return lya_fail(nullptr, LYA_ERR_CUDA, "lya_ctx_create: no CUDA device (%s)", cudaGetErrorString(e));
+  if (device < 0 || device >= ndev)
+    return lya_fail(nullptr, LYA_ERR_ARG, "lya_ctx_create: device %d out of range [0,%d)", device, ndev);
+  lya_ctx* ctx = new (std::nothrow) lya_ctx();
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ALLOC, "lya_ctx_create: host allocation failed");
+  ctx->device = device;
+  int rc = LYA_OK;
+  do {
+    if ((e = cudaSetDevice(device)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
+      rc = LYA_ERR_CUDA; break;
+    }
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = lya_alloc(&ctx->stats, ST_N)) != cudaSuccess) { rc = LYA_ERR_ALLOC; break; }
+  } while (0);
+  if (rc != LYA_OK) {
+    lya_fail(nullptr, rc, "lya_ctx_create: %s", cudaGetErrorString(e));
+    lya_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return LYA_OK;
+}
+
+extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
+  if (!ctx) return LYA_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  lya_free_catalog(ctx->cat);
+  lya_free_queue(ctx->wq);
+  lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LYA_OK;
+}
+
+extern "C" int lya_set_bins(lya_ctx* ctx, double rpmax, double rtmax, int32_t np, int32_t nt) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_set_bins: ctx is NULL");
+  if (!(rpmax > 0) || !(rtmax > 0) || np <= 0 || nt <= 0 || (int64_t)np * nt > LYA_MAX_BINS)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_set_bins: need rpmax, rtmax > 0 and 0 < np*nt <= %d (got %g %g %d %d)",
+                    LYA_MAX_BINS, rpmax, rtmax, np, nt);
+  ctx->rpmax = rpmax; ctx->rtmax = rtmax; ctx->np = np; ctx->nt = nt;
+  ctx->bins_set = true;
+  ctx->have_result = false;
+  return LYA_OK;
+}
+
+// ------------------------------------------------------------------ packing
+__global__ void k_pack(int64_t n, const int64_t* __restrict__ start, const int64_t* __restrict__ pstart,
+                       const double* __restrict__ dc, const double* __restrict__ w, const double* __restrict__ dw,
+                       const double* __restrict__ z, const double* __restrict__ dl, double* __restrict__ o_dc,
+                       double* __restrict__ o_w, double* __restrict__ o_dw, double* __restrict__ o_z,
+                       double* __restrict__ o_dl, double4* __restrict__ o_pix8, float4* __restrict__ o_pix4,
+                       float* __restrict__ o_z32,
+                       int32_t* __restrict__ o_len, uint8_t* __restrict__ o_sorted) {
+  for (int64_t f = blockIdx.x; f < n; f += gridDim.x) {
+    const int64_t s = start[f], L = start[f + 1] - s, d = pstart[f];
+    int ok = 1;
+    for (int64_t k = threadIdx.x; k < L; k += blockDim.x) {
+      const double x = dc[s + k];
+      o_dc[d + k] = x;
+      o_w[d + k] = w[s + k];
+      o_dw[d + k] = dw[s + k];
+      o_z[d + k] = z[s + k];
+      if (dl) o_dl[d + k] = dl[s + k];
+      o_pix8[d + k] = make_double4(x, w[s + k], dw[s + k], z[s + k]);
+      const float hi = __double2float_rn(x);
+      const float lo = __double2float_rn(x - (double)hi);
+      o_pix4[d + k] = make_float4(hi, lo, __double2float_rn(w[s + k]), __double2float_rn(dw[s + k]));
+      o_z32[d + k] = __double2float_rn(z[s + k]);
+      if (k + 1 < L && !(x <= dc[s + k + 1])) ok = 0;
+    }
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x == 0) {
+      o_len[f] = (int32_t)L;
+      o_sorted[f] = (uint8_t)ok;
+    }
+    __syncthreads();
+  }
+}
+
+extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start, const double* dc, const double* w,
+                                  const double* dw, const double* z, const double* dl, const double* ux,
+                                  const double* uy, const double* uz, const double* ra, const double* dec,
+                                  const int64_t* name, const int32_t* owner_slot, int32_t n_slots,
+                                  const double* omega, const double* odl2) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_upload_forests: ctx is NULL");
+  if (n < 0 || n >= (int64_t)INT32_MAX) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: bad n_forests %lld",
+                                                       (long long)n);
+  if (!start || (n > 0 && (!ux || !uy || !uz || !ra || !dec || !name || !owner_slot)))
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: required pointer is NULL");
+  if (n_slots < 0 || (n > 0 && n_slots == 0)) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: bad n_slots");
+  if (start[0] != 0) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: start[0] must be 0");
+  for (int64_t f = 0; f < n; ++f) {
+    if (start[f + 1] < start[f]) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: start not non-decreasing at %lld",
+                                                 (long long)f);
+    if (start[f + 1] - start[f] > 65536)
+      return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: forest %lld longer than 65536 pixels", (long long)f);
+    if (owner_slot[f] < 0 || owner_slot[f] >= n_slots)
+      return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: owner_slot[%lld]=%d outside [0,%d)", (long long)f,
+                      owner_slot[f], n_slots);
+    if (f > 0 && owner_slot[f] < owner_slot[f - 1])
+      return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: owner_slot must be non-decreasing (forest %lld)",
+                      (long long)f);
+  }
+  const int64_t npix = start[n];
+  if (npix > 0 && (!dc || !w || !dw || !z)) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: pixel array NULL");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  lya_free_catalog(ctx->cat);
+  lya_free_queue(ctx->wq);
+  ctx->have_result = false;
+
+  ctx->h_start.assign(start, start + n + 1);
+  ctx->h_slot.assign(owner_slot, owner_slot + n);
+  ctx->h_pstart.resize(n);
+  int64_t off = LYA_MARGIN;
+  for (int64_t f = 0; f < n; ++f) {
+    ctx->h_pstart[f] = off;
+    off += ((start[f + 1] - start[f]) + 3) & ~int64_t(3);
+  }
+  const int64_t npad = off + LYA_MARGIN;
+  DevCatalog& c = ctx->cat;
+  c.n = n; c.npix = npix; c.npad = npad; c.n_slots = n_slots;
+  c.has_dl = dl != nullptr;
+  c.has_moments = omega != nullptr && odl2 != nullptr;
+
+  cudaError_t e = cudaSuccess;
+#define ALLOC(p, cnt) if (e == cudaSuccess) e = lya_alloc(&(p), (size_t)(cnt))
+  ALLOC(c.pstart, n); ALLOC(c.len, n); ALLOC(c.sorted, n); ALLOC(c.slot, n);
+  ALLOC(c.ux, n); ALLOC(c.uy, n); ALLOC(c.uz, n); ALLOC(c.ra, n); ALLOC(c.dec, n); ALLOC(c.name, n);
+  ALLOC(c.omega, n); ALLOC(c.odl2, n);
+  ALLOC(c.dc, npad); ALLOC(c.w, npad); ALLOC(c.dw, npad); ALLOC(c.z, npad); ALLOC(c.dl, npad);
+  ALLOC(c.pix4, npad); ALLOC(c.z32, npad); ALLOC(c.pix8, npad);
+  double *t_dc = nullptr, *t_w = nullptr, *t_dw = nullptr, *t_z = nullptr, *t_dl = nullptr;
+  int64_t* t_start = nullptr;
+  ALLOC(t_dc, npix); ALLOC(t_w, npix); ALLOC(t_dw, npix); ALLOC(t_z, npix); ALLOC(t_start, n + 1);
+  if (dl) ALLOC(t_dl, npix);
+#undef ALLOC
+  auto cleanup_tmp = [&]() { lya_free(t_dc); lya_free(t_w); lya_free(t_dw); lya_free(t_z); lya_free(t_dl); lya_free(t_start); };
+  if (e != cudaSuccess) {
+    cleanup_tmp();
+    lya_free_catalog(ctx->cat);
+    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_upload_forests: device allocation failed (%s)", cudaGetErrorString(e));
+  }
+  cudaStream_t s = ctx->stream;
+  auto H2D = [&](void* d, const void* h, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
+  };
+  H2D(c.pstart, ctx->h_pstart.data(), sizeof(int64_t) * n);
+  H2D(c.slot, owner_slot, sizeof(int32_t) * n);
+  H2D(c.ux, ux, sizeof(double) * n); H2D(c.uy, uy, sizeof(double) * n); H2D(c.uz, uz, sizeof(double) * n);
+  H2D(c.ra, ra, sizeof(double) * n); H2D(c.dec, dec, sizeof(double) * n);
+  H2D(c.name, name, sizeof(int64_t) * n);
+  if (omega) H2D(c.omega, omega, sizeof(double) * n);
+  if (odl2) H2D(c.odl2, odl2, sizeof(double) * n);
+  H2D(t_start, start, sizeof(int64_t) * (n + 1));
+  H2D(t_dc, dc, sizeof(double) * npix); H2D(t_w, w, sizeof(double) * npix); H2D(t_dw, dw, sizeof(double) * npix);
+  H2D(t_z, z, sizeof(double) * npix);
+  if (dl) H2D(t_dl, dl, sizeof(double) * npix);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.dc, 0, sizeof(double) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.w, 0, sizeof(double) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.dw, 0, sizeof(double) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.z, 0, sizeof(double) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.dl, 0, sizeof(double) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.pix4, 0, sizeof(float4) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.z32, 0, sizeof(float) * npad, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.pix8, 0, sizeof(double4) * npad, s);
+  if (e == cudaSuccess && !omega) e = cudaMemsetAsync(c.omega, 0, sizeof(double) * n, s);
+  if (e == cudaSuccess && !odl2) e = cudaMemsetAsync(c.odl2, 0, sizeof(double) * n, s);
+  if (e == cudaSuccess && n > 0) {
+    int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
+    k_pack<<<blocks, 128, 0, s>>>(n, t_start, c.pstart, t_dc, t_w, t_dw, t_z, t_dl, c.dc, c.w, c.dw, c.z, c.dl,
+                                  c.pix8, c.pix4, c.z32, c.len, c.sorted);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cleanup_tmp();
+  if (e != cudaSuccess) {
+    lya_free_catalog(ctx->cat);
+    return lya_fail(ctx, LYA_ERR_CUDA, "lya_upload_forests: %s", cudaGetErrorString(e));
+  }
+  return LYA_OK;
+}
+
+// ------------------------------------------------------------------ work queue from the host
+__global__ void k_check_pairs(int64_t np, const int32_t* f1, const int32_t* f2, int64_t n, unsigned long long* err) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < np; k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = f1[k], b = f2[k];
+    if (a < 0 || a >= n || b < 0 || b >= n || (k > 0 && f1[k - 1] > a)) atomicAdd(err, 1ull);
+  }
+}
+
+extern "C" int lya_set_pairs(lya_ctx* ctx, int64_t n_pairs, const int32_t* f1, const int32_t* f2) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_set_pairs: ctx is NULL");
+  if (n_pairs < 0 || (n_pairs > 0 && (!f1 || !f2))) return lya_fail(ctx, LYA_ERR_ARG, "lya_set_pairs: bad arguments");
+  if (ctx->cat.n == 0 && n_pairs > 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_set_pairs: upload forests first");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  lya_free_queue(ctx->wq);
+  ctx->have_result = false;
+  WorkQueue& q = ctx->wq;
+  cudaError_t e = lya_alloc(&q.f1, n_pairs);
+  if (e == cudaSuccess) e = lya_alloc(&q.f2, n_pairs);
+  if (e != cudaSuccess) {
+    lya_free_queue(q);
+    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_set_pairs: device allocation failed");
+  }
+  double ref = 0.0;
+  for (int64_t k = 0; k < n_pairs; ++k) {
+    if (f1[k] < 0 || f1[k] >= ctx->cat.n || f2[k] < 0 || f2[k] >= ctx->cat.n) {
+      lya_free_queue(q);
+      return lya_fail(ctx, LYA_ERR_ARG, "lya_set_pairs: pair %lld references a forest outside [0,%lld)", (long long)k,
+                      (long long)ctx->cat.n);
+    }
+    if (k > 0 && f1[k] < f1[k - 1]) {
+      lya_free_queue(q);
+      return lya_fail(ctx, LYA_ERR_ARG, "lya_set_pairs: f1 must be non-decreasing (pair %lld)", (long long)k);
+    }
+    ref += (double)(ctx->h_start[f1[k] + 1] - ctx->h_start[f1[k]]) * (double)(ctx->h_start[f2[k] + 1] - ctx->h_start[f2[k]]);
+  }
+  q.n_pairs = n_pairs;
+  q.ref_pairs = ref;
+  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(q.f1, f1, sizeof(int32_t) * n_pairs, cudaMemcpyHostToDevice, ctx->stream));
+  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(q.f2, f2, sizeof(int32_t) * n_pairs, cudaMemcpyHostToDevice, ctx->stream));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return LYA_OK;
+}
+
+extern "C" int lya_get_pairs(lya_ctx* ctx, int32_t* f1, int32_t* f2) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_get_pairs: ctx is NULL");
+  const int64_t np = ctx->wq.n_pairs;
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (np > 0 && f1) LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(f1, ctx->wq.f1, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, ctx->stream));
+  if (np > 0 && f2) LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(f2, ctx->wq.f2, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, ctx->stream));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return LYA_OK;
+}
+
+// ------------------------------------------------------------------ results
+__global__ void k_combine(int64_t nslot, int nb, const double* __restrict__ hist, double* __restrict__ out) {
+  // hist: [slot][q][2][nb] (hi, lo) -> out [slot][q][nb] = hi + lo
+  const int64_t total = nslot * LYA_NQ * (int64_t)nb;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sq = k / nb, b = k - sq * nb;
+    out[k] = hist[(sq * 2) * nb + b] + hist[(sq * 2 + 1) * nb + b];
+  }
+}
+
+extern "C" int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double* hist, uint64_t* counts) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_corr_get: ctx is NULL");
+  if (!ctx->have_result) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_get: no result (call lya_corr_run first)");
+  if (slot_first < 0 || n < 0 || slot_first + (int64_t)n > ctx->hist_slots)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_get: slots [%d,%d) outside [0,%d)", slot_first, slot_first + n,
+                    ctx->hist_slots);
+  if (n == 0) return LYA_OK;
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nb = ctx->hist_nb;
+  if (hist) {
+    double* tmp = nullptr;
+    cudaError_t e = lya_alloc(&tmp, (size_t)n * LYA_NQ * nb);
+    if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_get: device allocation failed");
+    const double* src = ctx->hist + (size_t)slot_first * LYA_NQ * 2 * nb;
+    int blocks = (int)std::min<int64_t>(((int64_t)n * LYA_NQ * nb + 255) / 256, (int64_t)ctx->num_sms * 8);
+    k_combine<<<blocks, 256, 0, ctx->stream>>>(n, nb, src, tmp);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hist, tmp, sizeof(double) * (size_t)n * LYA_NQ * nb, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    lya_free(tmp);
+    if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_get: %s", cudaGetErrorString(e));
+  }
+  if (counts) {
+    LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(counts, ctx->counts + (size_t)slot_first * nb,
+                                        sizeof(unsigned long long) * (size_t)n * nb, cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+    LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return LYA_OK;
+}
+
+extern "C" int lya_stats(lya_ctx* ctx, lya_stats_t* out) {
+  if (!ctx || !out) return lya_fail(ctx, LYA_ERR_ARG, "lya_stats: NULL argument");
+  *out = ctx->last;
+  out->n_pairs = ctx->wq.n_pairs;
+  out->ref_pairs = ctx->wq.ref_pairs;
+  out->n_slots = ctx->cat.n_slots;
+  out->n_forests = (int32_t)ctx->cat.n;
+  return LYA_OK;
+}

@@ -1,0 +1,738 @@
+// Pair-binning kernels of the lya2pcf B200 library.
+//
+// Reference: pair_correlation (cuda_kernels.cpp:90-162), launched once per
+// forest by two_point_per_pixel (correlation_procedures_pycuda.py:141-166).
+// For every pixel pair (i in f1, j in f2) of a neighbouring forest pair:
+//   cos12 = x1*x2 + y1*y2 + z1*z2, ch = sqrt(0.5(1+cos12)), sh = sqrt(0.5(1-cos12))
+//   rp = |dc1-dc2| ch, rt = (dc1+dc2) sh, bp = floor(rp np/rpmax), bt = floor(rt nt/rtmax)
+//   in range: W[bp,bt] += w1 w2, DW[bp,bt] += dw1 dw2
+// plus the outputs the reference lacks: pair count, sum w1w2 rp, sum w1w2 rt,
+// sum w1w2 (z1+z2)/2.
+//
+// B200 design:
+// * One persistent launch over the whole work queue.  Each CTA owns a
+//   contiguous, cost-balanced range of forest pairs; its warps pull pairs from
+//   that range through a shared-memory counter.  Pairs are grouped by owner
+//   slot, so the CTA accumulates one slot at a time in a shared-memory FP64
+//   histogram and flushes it to global memory only when the slot changes,
+//   through compensated (hi, lo) FP64 atomics.
+// * A forest pair is walked along diagonals j - i = m (constant wavelength
+//   offset on a common grid).  Along a diagonal |dc1-dc2| and dc1+dc2 change
+//   slowly, so (bp, bt) stays constant for tens of steps: each lane keeps the
+//   running sums of its current bin in registers and touches shared memory only
+//   when the bin changes.  With sorted dc the walk is limited to the diagonal
+//   band that can reach rp < rpmax, and a diagonal stops once rt >= rtmax.
+// * FP32-guarded kernel: rp and rt are evaluated in FP32 from dc = hi + lo
+//   (two floats) with cos/sin of the half angle computed once per forest pair
+//   in FP64 exactly as the reference does.  A bin is accepted from FP32 only
+//   when both coordinates are at least `guard` (bin units) away from a bin edge;
+//   otherwise the pair is re-evaluated with the reference's FP64 formula.  The
+//   guard is checked on the host against a proven bound on the FP32 error, so
+//   every bin index (and hence every pair count) equals the FP64 formula's.
+#include <thrust/binary_search.h>
+#include <thrust/execution_policy.h>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/scan.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "lya_internal.cuh"
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+struct CorrParams {
+  const float4* __restrict__ pix4;
+  const double4* __restrict__ pix8;
+  const float* __restrict__ z32;
+  const double* __restrict__ dc;
+  const double* __restrict__ w;
+  const double* __restrict__ dw;
+  const double* __restrict__ z;
+  const int64_t* __restrict__ pstart;
+  const int32_t* __restrict__ len;
+  const uint8_t* __restrict__ sorted;
+  const int32_t* __restrict__ slot;
+  const double* __restrict__ ux;
+  const double* __restrict__ uy;
+  const double* __restrict__ uz;
+  const int32_t* __restrict__ f1;
+  const int32_t* __restrict__ f2;
+  const int64_t* __restrict__ cta_begin;
+  double binner_rp, binner_rt;
+  double inv_binner_rp, inv_binner_rt;
+  int np, nt, nb;
+  float gx, gy;        // guard half-widths in bin units (FP32 kernel)
+  int cos_variant;
+  int run_cap;
+  double* hist;                 // [slot][LYA_NQ][2][nb]
+  unsigned long long* counts;   // [slot][nb]
+  unsigned long long* stats;    // [ST_N]
+};
+
+struct LaneStats {
+  unsigned long long evaluated = 0, recheck = 0, runs = 0, inrange = 0;
+};
+
+// Shared-memory histogram of the slot being accumulated.
+struct SmemHist {
+  double* q;                  // [LYA_NQ][nb]
+  unsigned long long* n;      // [nb]
+};
+
+__device__ __forceinline__ void pair_half_angles(const CorrParams& p, int a, int b, double& ch, double& sh) {
+  double c = lya_cos12(p.ux[a], p.uy[a], p.uz[a], p.ux[b], p.uy[b], p.uz[b], p.cos_variant);
+  // Rounding can push cos12 past 1 for coincident lines of sight; the
+  // reference then takes sqrt of a negative number.  Clamp: rt = 0.
+  c = fmin(1.0, fmax(-1.0, c));
+  ch = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(1.0, c)));
+  sh = __dsqrt_rn(__dmul_rn(0.5, __dsub_rn(1.0, c)));
+}
+
+// Exact FP64 bin of a pixel pair (the reference formula); -1 when out of range.
+__device__ __forceinline__ int bin_fp64(const CorrParams& p, double d1, double d2, double ch, double sh,
+                                        double& rp, double& rt) {
+  rp = __dmul_rn(fabs(__dsub_rn(d1, d2)), ch);
+  rt = __dmul_rn(__dadd_rn(d1, d2), sh);
+  const double fp = floor(__dmul_rn(rp, p.binner_rp));
+  const double ft = floor(__dmul_rn(rt, p.binner_rt));
+  if (fp >= 0.0 && fp < (double)p.np && ft >= 0.0 && ft < (double)p.nt) return (int)fp * p.nt + (int)ft;
+  return -1;
+}
+
+// Diagonal band [m_lo, m_hi] of a forest pair with sorted dc: every pixel pair
+// that can land in range has m = j - i inside it.  hi2(j) returns f2's dc_hi.
+template <typename HiLoad>
+__device__ void diagonal_band(int L1, int L2, const float4* __restrict__ P1, HiLoad hi2, double rp_reach,
+                              double rt_reach, int& m_lo, int& m_hi) {
+  const int lane = threadIdx.x & 31;
+  int lo = INT_MAX, hi = INT_MIN;
+  for (int i = lane; i < L1; i += 32) {
+    const double d1 = (double)P1[i].x;
+    const double margin = 1e-3 + 1e-6 * fabs(d1);
+    const double tlo = d1 - rp_reach - margin;
+    const double thi = fmin(d1 + rp_reach, rt_reach - d1) + margin;
+    // first j with hi2[j] > tlo
+    int a = 0, b = L2;
+    while (a < b) { int mid = (a + b) >> 1; if ((double)hi2(mid) > tlo) b = mid; else a = mid + 1; }
+    const int jlo = a;
+    // last j with hi2[j] < thi
+    a = jlo; b = L2;
+    while (a < b) { int mid = (a + b) >> 1; if ((double)hi2(mid) < thi) a = mid + 1; else b = mid; }
+    const int jhi = a - 1;
+    if (jlo <= jhi) {
+      lo = min(lo, jlo - i);
+      hi = max(hi, jhi - i);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(FULL, lo, o));
+    hi = max(hi, __shfl_xor_sync(FULL, hi, o));
+  }
+  m_lo = lo;
+  m_hi = hi;
+}
+
+// ------------------------------------------------------------------ run records
+// A lane's run (consecutive pairs of one diagonal in one bin) ends when the bin
+// changes.  The lane appends the run's sums to its warp's record buffer in
+// shared memory (plain stores, positions from a ballot); the warp drains the
+// buffer into the CTA histogram with all 32 lanes when it holds 32 records or
+// more, so the long-latency FP64 shared atomics never run in a divergent branch.
+constexpr int REC = 64;
+
+struct __align__(16) RecF32 {
+  int bin, n;
+  float aw, adw, ax, ay, az, pad;
+};
+struct __align__(16) RecF64 {
+  int bin, n;
+  double aw, adw, ax, ay, az;
+};
+
+template <typename Rec>
+__device__ __forceinline__ void drain(Rec* buf, int cnt, const SmemHist& h, int nb, LaneStats& st) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  for (int k = lane; k < cnt; k += 32) {
+    const Rec r = buf[k];
+    st.runs++;
+    st.inrange += (unsigned long long)r.n;
+    atomicAdd(&h.q[0 * nb + r.bin], (double)r.aw);
+    atomicAdd(&h.q[1 * nb + r.bin], (double)r.adw);
+    atomicAdd(&h.q[2 * nb + r.bin], (double)r.ax);
+    atomicAdd(&h.q[3 * nb + r.bin], (double)r.ay);
+    atomicAdd(&h.q[4 * nb + r.bin], (double)r.az);
+    atomicAdd(&h.n[r.bin], (unsigned long long)r.n);
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------ diagonal walk
+// Lane layout: the 32 lanes of a warp walk 32 diagonals m = mg + 2*lane (two
+// passes, mg even/odd offsets, cover a block of 64 diagonals) placed on one
+// anti-diagonal: at step k lane l holds the pair (i, j) = (base+k-l, base+k+mg+l).
+// Every lane then has the same i + j, hence nearly the same dc1 + dc2 and the
+// same rt: rt-bin crossings and the rtmax stop happen for the whole warp at
+// once.  rp-bin crossings (|dc1-dc2| drifts slowly along a diagonal) are
+// handled by shifting the run's bin by +-1 in rp, without re-deriving it.
+//
+// Run state of a lane: bin (bx, by; bx < 0 = out of range), its acceptance
+// interval [xlo, xhi) x [ylo, yhi) in bin units, the step k0 the run started
+// and the running sums.  Traits supply the arithmetic precision.
+
+struct TrF32 {
+  using Real = float;
+  using Rec = RecF32;
+  struct Pix { float4 q; float z; };
+  struct Geo { float chb, shb; };
+  struct Ptr { const float4* __restrict__ q; const float* __restrict__ z; };
+  static __device__ __forceinline__ Ptr ptr(const CorrParams& p, int64_t off) { return Ptr{p.pix4 + off, p.z32 + off}; }
+  static __device__ __forceinline__ Pix load(const Ptr& a, int k) {
+    Pix v;
+    v.q = a.q[k];
+    v.z = a.z[k];
+    return v;
+  }
+  static __device__ __forceinline__ void coords(const Geo& g, const Pix& a, const Pix& b, float& x, float& y,
+                                                float&, float&) {
+    x = fabsf((a.q.x - b.q.x) + (a.q.y - b.q.y)) * g.chb;
+    y = (a.q.x + b.q.x) * g.shb;
+  }
+  struct Acc {
+    float aw, adw, ax, ay, az;
+    __device__ __forceinline__ void zero() { aw = adw = ax = ay = az = 0.f; }
+    __device__ __forceinline__ void add(const Pix& a, const Pix& b, float x, float y, float, float) {
+      const float w12 = a.q.z * b.q.z;
+      aw += w12;
+      adw = fmaf(a.q.w, b.q.w, adw);
+      ax = fmaf(w12, x, ax);
+      ay = fmaf(w12, y, ay);
+      az = fmaf(w12, a.z + b.z, az);
+    }
+  };
+};
+
+struct TrF64 {
+  using Real = double;
+  using Rec = RecF64;
+  using Pix = double4;   // (dc, w, dw, z)
+  struct Geo { double ch, sh, brp, brt; };
+  using Ptr = const double4* __restrict__;
+  static __device__ __forceinline__ Ptr ptr(const CorrParams& p, int64_t off) { return p.pix8 + off; }
+  static __device__ __forceinline__ Pix load(Ptr a, int k) { return a[k]; }
+  static __device__ __forceinline__ void coords(const Geo& g, const Pix& a, const Pix& b, double& x, double& y,
+                                                double& rp, double& rt) {
+    rp = __dmul_rn(fabs(__dsub_rn(a.x, b.x)), g.ch);
+    rt = __dmul_rn(__dadd_rn(a.x, b.x), g.sh);
+    x = __dmul_rn(rp, g.brp);
+    y = __dmul_rn(rt, g.brt);
+  }
+  struct Acc {
+    double aw, adw, ax, ay, az;
+    __device__ __forceinline__ void zero() { aw = adw = ax = ay = az = 0.0; }
+    __device__ __forceinline__ void add(const Pix& a, const Pix& b, double, double, double rp, double rt) {
+      const double w12 = __dmul_rn(a.y, b.y);
+      aw += w12;
+      adw = __fma_rn(a.z, b.z, adw);
+      ax = __fma_rn(w12, rp, ax);
+      ay = __fma_rn(w12, rt, ay);
+      az = __fma_rn(w12, __dadd_rn(a.w, b.w), az);
+    }
+  };
+};
+
+template <class Real>
+struct Run {
+  int bx, by, k0;
+  Real xlo, xhi, ylo, yhi;
+};
+
+template <class Real>
+__device__ __forceinline__ Real inf_of();
+template <>
+__device__ __forceinline__ float inf_of<float>() { return __int_as_float(0x7f800000); }
+template <>
+__device__ __forceinline__ double inf_of<double>() { return __longlong_as_double(0x7ff0000000000000ll); }
+
+// Full classification of the pair starting a run.  FP32: accept the FP32 bin
+// when both coordinates are at least the guard away from a bin edge (the edge
+// at 0 cannot be crossed); otherwise take the bin from the reference FP64
+// formula (d1p/d2p point at the pixels' FP64 data).  FP64: exact floor.
+template <class Real>
+__device__ __forceinline__ void classify(const CorrParams& p, Run<Real>& r, Real x, Real y, Real gx, Real gy,
+                                         const double4* __restrict__ d1p, const double4* __restrict__ d2p,
+                                         double ch, double sh, LaneStats& st) {
+  const Real INF = inf_of<Real>();
+  const Real npf = (Real)p.np, ntf = (Real)p.nt;
+  if (!(x >= (Real)0) || !(y >= (Real)0)) {  // NaN or negative: excluded, re-examined every step
+    r.bx = -1; r.by = -1; r.xlo = INF; r.xhi = -INF; r.ylo = INF; r.yhi = -INF;
+    return;
+  }
+  if (y >= ntf + gy) {  // clearly beyond rtmax
+    r.bx = -1; r.by = -1; r.xlo = -INF; r.xhi = INF; r.ylo = ntf + gy; r.yhi = INF;
+    return;
+  }
+  if (x >= npf + gx) {  // clearly beyond rpmax
+    r.bx = -1; r.by = -1; r.xlo = npf + gx; r.xhi = INF; r.ylo = -INF; r.yhi = INF;
+    return;
+  }
+  const Real fx = floor(x), fy = floor(y);
+  const bool safe = (fx == (Real)0 || x - fx >= gx) && (fx + (Real)1 - x > gx) &&
+                    (fy == (Real)0 || y - fy >= gy) && (fy + (Real)1 - y > gy);
+  if (safe) {
+    r.xlo = fx == (Real)0 ? -INF : fx + gx; r.xhi = fx + (Real)1 - gx;
+    r.ylo = fy == (Real)0 ? -INF : fy + gy; r.yhi = fy + (Real)1 - gy;
+    if (fx < npf && fy < ntf) { r.bx = (int)fx; r.by = (int)fy; }
+    else { r.bx = -1; r.by = -1; }
+    return;
+  }
+  // FP32 only (gx = gy = 0 makes every FP64 pair safe): inside the guard band
+  // the reference FP64 formula decides; the next pair is classified again.
+  double rp, rt;
+  const int k = bin_fp64(p, d1p->x, d2p->x, ch, sh, rp, rt);
+  if (k >= 0) { r.bx = k / p.nt; r.by = k - r.bx * p.nt; } else { r.bx = -1; r.by = -1; }
+  r.xlo = INF; r.xhi = -INF; r.ylo = INF; r.yhi = -INF;
+  st.recheck++;
+}
+
+template <class Tr>
+__device__ __forceinline__ void put_record(typename Tr::Rec* buf, int pos, int bin, int n, const typename Tr::Acc& a) {
+  typename Tr::Rec rec;
+  rec.bin = bin; rec.n = n; rec.aw = a.aw; rec.adw = a.adw; rec.ax = a.ax; rec.ay = a.ay; rec.az = a.az;
+  buf[pos] = rec;
+}
+
+// Close the runs of the lanes in `who` at step k (records for in-range runs).
+template <class Tr>
+__device__ __forceinline__ void close_runs(bool who, Run<typename Tr::Real>& r, const typename Tr::Acc& acc, int k,
+                                           int nt, typename Tr::Rec* buf, int& cnt, unsigned lt, LaneStats& st) {
+  const bool wr = who && r.bx >= 0 && k > r.k0;
+  const unsigned rb = __ballot_sync(FULL, wr);
+  if (wr) put_record<Tr>(buf, cnt + __popc(rb & lt), r.bx * nt + r.by, k - r.k0, acc);
+  cnt += __popc(rb);
+}
+
+template <class Tr, bool GUARDED>
+__device__ void item_diag(const CorrParams& p, int64_t t, const SmemHist& h, typename Tr::Rec* buf, int& cnt,
+                          LaneStats& st) {
+  using Real = typename Tr::Real;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int fa = p.f1[t], fb = p.f2[t];
+  const int L1 = p.len[fa], L2 = p.len[fb];
+  if (L1 <= 0 || L2 <= 0) return;
+  const int64_t a = p.pstart[fa], b = p.pstart[fb];
+  const int np = p.np, nt = p.nt, nb = p.nb;
+  double ch, sh;
+  pair_half_angles(p, fa, fb, ch, sh);
+  typename Tr::Geo geo;
+  if constexpr (GUARDED) {
+    geo.chb = __double2float_rn(ch * p.binner_rp);
+    geo.shb = __double2float_rn(sh * p.binner_rt);
+  } else {
+    geo.ch = ch; geo.sh = sh; geo.brp = p.binner_rp; geo.brt = p.binner_rt;
+  }
+  const Real gx = GUARDED ? (Real)p.gx : (Real)0, gy = GUARDED ? (Real)p.gy : (Real)0;
+  const bool srt = p.sorted[fa] && p.sorted[fb];
+  int m_lo = -(L1 - 1), m_hi = L2 - 1;
+  if (srt) {
+    const float4* __restrict__ P1 = p.pix4 + a;
+    const float4* __restrict__ P2 = p.pix4 + b;
+    const double slack = GUARDED ? 2.0 * p.gx : 1e-3;
+    const double rp_reach = ch > 0.0 ? ((double)np + slack) / (ch * p.binner_rp) : 1e300;
+    const double rt_reach = sh > 0.0 ? ((double)nt + slack) / (sh * p.binner_rt) : 1e300;
+    diagonal_band(L1, L2, P1, [&](int j) { return P2[j].x; }, rp_reach, rt_reach, m_lo, m_hi);
+  }
+  const Real INF = inf_of<Real>();
+  const Real ycut = (Real)nt + gy;
+  const int cap = p.run_cap;   // power of two
+  for (int mb = m_lo; mb <= m_hi; mb += 64) {
+    for (int par = 0; par < 2; ++par) {
+      const int mg = mb + par;
+      const int m = mg + 2 * lane;
+      const int i_lo = max(0, -m);
+      const int i_hi = (m <= m_hi) ? min(L1, L2 - m) : i_lo;
+      const bool nonempty = i_lo < i_hi;
+      int base = nonempty ? i_lo + lane : INT_MAX;
+      for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
+      if (base == INT_MAX) continue;
+      const int k_beg = i_lo + lane - base;           // lane's first step
+      int stop = nonempty ? i_hi + lane - base : 0;   // lane's end (exclusive), shrinks on the rtmax stop
+      int k_end = stop;
+      for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
+      const int ioff = base - lane;            // i = ioff + k   (>= -31)
+      const int joff = base + mg + lane;       // j = joff + k   (>= -31)
+      // lane pointers at step 0; loads run up to 34 pixels outside a forest,
+      // which stays inside the LYA_MARGIN-padded arrays
+      const typename Tr::Ptr A1 = Tr::ptr(p, a + ioff);
+      const typename Tr::Ptr A2 = Tr::ptr(p, b + joff);
+      Run<Real> r;
+      r.bx = -1; r.by = -1; r.k0 = 0; r.xlo = INF; r.xhi = -INF; r.ylo = INF; r.yhi = -INF;
+      typename Tr::Acc acc;
+      acc.zero();
+      typename Tr::Pix q1 = Tr::load(A1, 0), q2 = Tr::load(A2, 0);
+#pragma unroll 2
+      for (int k = 0; k < k_end; ++k) {
+        const typename Tr::Pix n1 = Tr::load(A1, k + 1), n2 = Tr::load(A2, k + 1);
+        bool act = k >= k_beg && k < stop;
+        Real x, y, rp, rt;
+        Tr::coords(geo, q1, q2, x, y, rp, rt);
+        const bool exl = x < r.xlo, exh = !(x < r.xhi), eyl = y < r.ylo, eyh = !(y < r.yhi);
+        const bool slow = act && (exl || exh || eyl || eyh);
+        if (__any_sync(FULL, slow)) {
+          close_runs<Tr>(slow, r, acc, k, nt, buf, cnt, lt, st);
+          if (slow) {
+            acc.zero();
+            r.k0 = k;
+            bool full = true;
+            // rp crossing into the adjacent bin, rt unchanged: shift the run by one in rp
+            if (!eyl && !eyh && r.bx >= 0) {
+              const int nbx = exh ? r.bx + 1 : r.bx - 1;
+              const Real d = exh ? (Real)1 : (Real)-1;
+              const Real nlo = r.xlo + d, nhi = r.xhi + d;
+              if (nbx >= 0 && nbx < np && x >= nlo && x < nhi) {
+                r.bx = nbx; r.xlo = nlo; r.xhi = nhi;
+                full = false;
+              }
+            }
+            if (full) {
+              if (srt && y >= ycut) {   // rt only grows along a sorted diagonal: lane done
+                stop = k;
+                act = false;
+                r.bx = -1;
+              } else {
+                classify<Real>(p, r, x, y, gx, gy, p.pix8 + a + ioff + k, p.pix8 + b + joff + k, ch, sh, st);
+              }
+            }
+          }
+          if (cnt > REC - 32) {
+            drain(buf, cnt, h, nb, st);
+            cnt = 0;
+          }
+        }
+        if (act) acc.add(q1, q2, x, y, rp, rt);
+        q1 = n1;
+        q2 = n2;
+        if ((k & (cap - 1)) == cap - 1) {   // bound the length of a register sum
+          const bool live = k >= k_beg && k < stop;
+          close_runs<Tr>(live, r, acc, k + 1, nt, buf, cnt, lt, st);
+          if (live) { acc.zero(); r.k0 = k + 1; }
+          if (cnt > REC - 32) {
+            drain(buf, cnt, h, nb, st);
+            cnt = 0;
+          }
+          if (__all_sync(FULL, k + 1 >= stop)) break;
+        }
+      }
+      st.evaluated += (unsigned long long)max(0, min(stop, k_end) - k_beg);
+      const int kfin = min(stop, k_end);
+      close_runs<Tr>(true, r, acc, max(kfin, r.k0), nt, buf, cnt, lt, st);
+      if (cnt > REC - 32) {
+        drain(buf, cnt, h, nb, st);
+        cnt = 0;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ FP64 plain (every pixel pair)
+__device__ void item_plain(const CorrParams& p, int64_t t, const SmemHist& h, LaneStats& st) {
+  const int lane = threadIdx.x & 31;
+  const int fa = p.f1[t], fb = p.f2[t];
+  const int L1 = p.len[fa], L2 = p.len[fb];
+  if (L1 <= 0 || L2 <= 0) return;
+  const int64_t a = p.pstart[fa], b = p.pstart[fb];
+  double ch, sh;
+  pair_half_angles(p, fa, fb, ch, sh);
+  for (int i = 0; i < L1; ++i) {
+    const double4 q1 = p.pix8[a + i];
+    for (int j = lane; j < L2; j += 32) {
+      const double4 q2 = p.pix8[b + j];
+      double rp, rt;
+      const int k = bin_fp64(p, q1.x, q2.x, ch, sh, rp, rt);
+      st.evaluated++;
+      if (k >= 0) {
+        const double w12 = __dmul_rn(q1.y, q2.y);
+        atomicAdd(&h.q[0 * p.nb + k], w12);
+        atomicAdd(&h.q[1 * p.nb + k], __dmul_rn(q1.z, q2.z));
+        atomicAdd(&h.q[2 * p.nb + k], __dmul_rn(w12, rp));
+        atomicAdd(&h.q[3 * p.nb + k], __dmul_rn(w12, rt));
+        atomicAdd(&h.q[4 * p.nb + k], __dmul_rn(w12, __dadd_rn(q1.w, q2.w)));
+        atomicAdd(&h.n[k], 1ull);
+        st.inrange++;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ persistent driver
+// Compensated accumulation of v into the (hi, lo) pair at hi/lo: the atomic
+// returns the old hi, the rounding error of hi + v is recovered exactly
+// (TwoSum) and added to lo.
+__device__ __forceinline__ void add_compensated(double* hi, double* lo, double v) {
+  const double old = atomicAdd(hi, v);
+  const double s = old + v;
+  const double bb = s - old;
+  const double err = (old - (s - bb)) + (v - bb);
+  if (err != 0.0) atomicAdd(lo, err);
+}
+
+template <int KIND>
+constexpr size_t rec_bytes() {
+  return KIND == LYA_KERNEL_FP32_GUARDED ? sizeof(RecF32) : (KIND == LYA_KERNEL_FP64_DIAGONAL ? sizeof(RecF64) : 0);
+}
+
+template <int KIND, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nb = p.nb;
+  SmemHist h;
+  h.q = reinterpret_cast<double*>(smem);
+  h.n = reinterpret_cast<unsigned long long*>(h.q + LYA_NQ * nb);
+  unsigned char* bufs = reinterpret_cast<unsigned char*>(h.n + nb);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* mybuf = bufs + (size_t)warp * REC * rec_bytes<KIND>();
+  __shared__ unsigned long long s_next;
+  __shared__ long long s_seg_end;
+  __shared__ int s_slot;
+
+  for (int k = threadIdx.x; k < LYA_NQ * nb; k += blockDim.x) h.q[k] = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) h.n[k] = 0ull;
+  LaneStats st;
+  int cnt = 0;   // records pending in this warp's buffer (warp-uniform)
+  const int64_t begin = p.cta_begin[blockIdx.x], end = p.cta_begin[blockIdx.x + 1];
+  int64_t seg = begin;
+  __syncthreads();
+  while (seg < end) {
+    if (threadIdx.x == 0) {
+      const int s = p.slot[p.f1[seg]];
+      int64_t lo = seg + 1, hi = end;   // first item of a later slot
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (p.slot[p.f1[mid]] > s) hi = mid; else lo = mid + 1;
+      }
+      s_seg_end = lo;
+      s_slot = s;
+      s_next = (unsigned long long)seg;
+    }
+    __syncthreads();
+    const int64_t seg_end = s_seg_end;
+    const int slot = s_slot;
+    for (;;) {
+      unsigned long long t = 0;
+      if (lane == 0) t = atomicAdd(&s_next, 1ull);
+      t = __shfl_sync(FULL, t, 0);
+      if ((int64_t)t >= seg_end) break;
+      if (KIND == LYA_KERNEL_FP32_GUARDED)
+        item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+      else if (KIND == LYA_KERNEL_FP64_DIAGONAL)
+        item_diag<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
+      else item_plain(p, (int64_t)t, h, st);
+    }
+    if (KIND == LYA_KERNEL_FP32_GUARDED) drain(reinterpret_cast<RecF32*>(mybuf), cnt, h, nb, st);
+    if (KIND == LYA_KERNEL_FP64_DIAGONAL) drain(reinterpret_cast<RecF64*>(mybuf), cnt, h, nb, st);
+    cnt = 0;
+    __syncthreads();
+    double* gh = p.hist + (size_t)slot * LYA_NQ * 2 * nb;
+    for (int k = threadIdx.x; k < LYA_NQ * nb; k += blockDim.x) {
+      const int q = k / nb, bb = k - q * nb;
+      double v = h.q[k];
+      if (v != 0.0) {
+        // the FP32 kernel sums w12*x in bin units; all kernels sum w12*(z1+z2)
+        if (KIND == LYA_KERNEL_FP32_GUARDED && q == 2) v *= p.inv_binner_rp;
+        if (KIND == LYA_KERNEL_FP32_GUARDED && q == 3) v *= p.inv_binner_rt;
+        if (q == 4) v *= 0.5;
+        add_compensated(gh + (size_t)(q * 2) * nb + bb, gh + (size_t)(q * 2 + 1) * nb + bb, v);
+      }
+      h.q[k] = 0.0;
+    }
+    unsigned long long* gc = p.counts + (size_t)slot * nb;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      if (h.n[k]) atomicAdd(&gc[k], h.n[k]);
+      h.n[k] = 0ull;
+    }
+    __syncthreads();
+    seg = seg_end;
+  }
+  // statistics: one atomic per warp
+  unsigned long long e = st.evaluated, r = st.recheck, u = st.runs, n = st.inrange;
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_xor_sync(FULL, e, o);
+    r += __shfl_xor_sync(FULL, r, o);
+    u += __shfl_xor_sync(FULL, u, o);
+    n += __shfl_xor_sync(FULL, n, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&p.stats[ST_EVALUATED], e);
+    atomicAdd(&p.stats[ST_RECHECK], r);
+    atomicAdd(&p.stats[ST_RUNS], u);
+    atomicAdd(&p.stats[ST_INRANGE], n);
+  }
+}
+
+template <int KIND, int WARPS>
+cudaError_t launch_corr(const CorrParams& p, int nctas, int nb, cudaStream_t s) {
+  const size_t smem = (size_t)nb * (LYA_NQ * sizeof(double) + sizeof(unsigned long long)) +
+                      (size_t)WARPS * REC * rec_bytes<KIND>();
+  cudaError_t e = cudaFuncSetAttribute(k_corr<KIND, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_corr<KIND, WARPS><<<nctas, WARPS * 32, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ CTA ranges
+__global__ void k_item_cost(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ f2,
+                            const int32_t* __restrict__ len, long long* __restrict__ cost) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    cost[k] = (long long)len[f1[k]] * (long long)len[f2[k]] + 64;   // + fixed per-pair overhead
+}
+
+__global__ void k_cta_bounds(int nctas, int64_t n, const long long* __restrict__ prefix, int64_t* __restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > nctas) return;
+  if (b == 0) { out[0] = 0; return; }
+  if (b == nctas || n == 0) { out[b] = n; return; }
+  const double total = (double)prefix[n - 1];
+  const long long target = (long long)(total * ((double)b / nctas));
+  int64_t lo = 0, hi = n;   // first k with prefix[k] > target
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (prefix[mid] > target) hi = mid; else lo = mid + 1;
+  }
+  out[b] = lo;
+}
+
+}  // namespace
+
+int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out) {
+  const int64_t n = ctx->wq.n_pairs;
+  long long* cost = nullptr;
+  cudaError_t e = lya_alloc(&cost, (size_t)std::max<int64_t>(n, 1));
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "cta ranges: allocation failed");
+  if (n > 0) {
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 16);
+    k_item_cost<<<blocks, 256, 0, ctx->stream>>>(n, ctx->wq.f1, ctx->wq.f2, ctx->cat.len, cost);
+    thrust::inclusive_scan(thrust::cuda::par.on(ctx->stream), cost, cost + n, cost);
+  }
+  k_cta_bounds<<<(nctas + 1 + 127) / 128, 128, 0, ctx->stream>>>(nctas, n, cost, d_out);
+  e = cudaGetLastError();
+  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  lya_free(cost);
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return lya_fail(ctx, LYA_ERR_CUDA, "cta ranges: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  return LYA_OK;
+}
+
+// Largest FP32 error of a bin coordinate (bin units) for coordinates below
+// `reach` bins: four roundings of relative size 2^-24 (hi-difference and lo sum,
+// the FP32 factor ch*binner, the product) bound |x - x64| by 2^-22 x; the
+// FP64 reference value itself carries < 2^-51 x.  Margin 10%, plus the
+// rounding of the interval ends fx + guard in FP32 (half an ulp of reach).
+static double guard_bound_bins(double reach) {
+  const double rel = std::ldexp(1.0, -22) + std::ldexp(1.0, -50);
+  const double ulp_reach = std::ldexp(1.0, (int)std::floor(std::log2(std::max(reach, 1.0))) - 23);
+  return 1.1 * rel * reach + ulp_reach + 1e-12;
+}
+
+int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
+  const int kind = o->kernel;
+  const int nb = ctx->np * ctx->nt;
+  const int nslots = ctx->cat.n_slots;
+  cudaStream_t s = ctx->stream;
+
+  // guard check (FP32 kernel)
+  const double gx_bins = o->guard * ctx->np / ctx->rpmax;
+  const double gy_bins = o->guard * ctx->nt / ctx->rtmax;
+  const double bx = guard_bound_bins(ctx->np + 1.0), by = guard_bound_bins(ctx->nt + 1.0);
+  ctx->last.guard_bound = std::max(bx * ctx->rpmax / ctx->np, by * ctx->rtmax / ctx->nt);
+  if (kind == LYA_KERNEL_FP32_GUARDED && (!(gx_bins >= bx) || !(gy_bins >= by) || gx_bins > 0.25 || gy_bins > 0.25))
+    return lya_fail(ctx, LYA_ERR_GUARD,
+                    "guard %.3g Mpc/h outside [%.3g, %.3g]: below the proven FP32 error bound or above a quarter bin",
+                    o->guard, ctx->last.guard_bound, 0.25 * std::min(ctx->rpmax / ctx->np, ctx->rtmax / ctx->nt));
+
+  // outputs
+  if (ctx->hist_slots != nslots || ctx->hist_nb != nb || !ctx->hist) {
+    lya_free(ctx->hist); lya_free(ctx->counts);
+    cudaError_t e = lya_alloc(&ctx->hist, (size_t)nslots * LYA_NQ * 2 * nb);
+    if (e == cudaSuccess) e = lya_alloc(&ctx->counts, (size_t)nslots * nb);
+    if (e != cudaSuccess) {
+      lya_free(ctx->hist); lya_free(ctx->counts);
+      ctx->hist_slots = 0;
+      return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_run: output allocation failed");
+    }
+    ctx->hist_slots = nslots; ctx->hist_nb = nb;
+  }
+  LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->hist, 0, sizeof(double) * (size_t)nslots * LYA_NQ * 2 * nb, s));
+  LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->counts, 0, sizeof(unsigned long long) * (size_t)nslots * nb, s));
+  LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->stats, 0, sizeof(unsigned long long) * ST_N, s));
+
+  const int warps = o->warps_per_block == 32 ? 32 : 16;
+  const int nctas = ctx->num_sms * std::max(1, o->blocks_per_sm);
+  if (ctx->cta_cap < nctas + 1) {
+    lya_free(ctx->cta_begin);
+    if (lya_alloc(&ctx->cta_begin, (size_t)nctas + 1) != cudaSuccess)
+      return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_run: allocation failed");
+    ctx->cta_cap = nctas + 1;
+  }
+  int rc = lya_prepare_cta_ranges(ctx, nctas, ctx->cta_begin);
+  if (rc != LYA_OK) return rc;
+
+  CorrParams p;
+  const DevCatalog& c = ctx->cat;
+  p.pix4 = c.pix4; p.z32 = c.z32; p.pix8 = c.pix8; p.dc = c.dc; p.w = c.w; p.dw = c.dw; p.z = c.z;
+  p.pstart = c.pstart; p.len = c.len; p.sorted = c.sorted; p.slot = c.slot;
+  p.ux = c.ux; p.uy = c.uy; p.uz = c.uz;
+  p.f1 = ctx->wq.f1; p.f2 = ctx->wq.f2; p.cta_begin = ctx->cta_begin;
+  p.binner_rp = (double)ctx->np / ctx->rpmax;
+  p.binner_rt = (double)ctx->nt / ctx->rtmax;
+  p.inv_binner_rp = ctx->rpmax / (double)ctx->np;
+  p.inv_binner_rt = ctx->rtmax / (double)ctx->nt;
+  p.np = ctx->np; p.nt = ctx->nt; p.nb = nb;
+  p.gx = (float)gx_bins; p.gy = (float)gy_bins;
+  p.cos_variant = ctx->cos_variant;
+  p.run_cap = 128;
+  p.hist = ctx->hist; p.counts = ctx->counts; p.stats = ctx->stats;
+
+  cudaError_t e = cudaSuccess;
+  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+  (void)warps;
+  if (kind == LYA_KERNEL_FP32_GUARDED)
+    e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16>(p, nctas, nb, s);
+  else if (kind == LYA_KERNEL_FP64_DIAGONAL)
+    e = launch_corr<LYA_KERNEL_FP64_DIAGONAL, 16>(p, nctas, nb, s);
+  else
+    e = launch_corr<LYA_KERNEL_FP64_PLAIN, 16>(p, nctas, nb, s);
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run launch: %s", cudaGetErrorString(e));
+  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+  unsigned long long hst[ST_N];
+  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(hst, ctx->stats, sizeof(hst), cudaMemcpyDeviceToHost, s));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  float ms = 0.f;
+  LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->last.kernel_ms = ms;
+  ctx->last.evaluated_pairs = (double)hst[ST_EVALUATED];
+  ctx->last.guard_rechecks = (double)hst[ST_RECHECK];
+  ctx->last.runs_flushed = (double)hst[ST_RUNS];
+  ctx->last.in_range_pairs = (double)hst[ST_INRANGE];
+  ctx->have_result = true;
+  return LYA_OK;
+}
+
+extern "C" int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_corr_run: ctx is NULL");
+  lya_corr_opts o{};
+  o.kernel = LYA_KERNEL_FP32_GUARDED;
+  o.guard = 1e-4;
+  if (opts) o = *opts;
+  if (o.kernel < 0 || o.kernel > 2) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: unknown kernel %d", o.kernel);
+  if (o.blocks_per_sm < 0 || o.blocks_per_sm > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: blocks_per_sm must be 0 or 1");
+  if (o.warps_per_block != 0 && o.warps_per_block != 16)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: warps_per_block must be 0 or 16");
+  if (!ctx->bins_set) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_run: call lya_set_bins first");
+  if (ctx->cat.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_run: no forests uploaded");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  return lya_corr_launch(ctx, &o);
+}

@@ -1,0 +1,141 @@
+// Internal declarations of the lya2pcf B200 library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "lya2pcf.h"
+
+#define LYA_MAX_BINS 4096
+#define LYA_WARP 32
+// Zero pixels before the first and after the last forest of the padded pixel
+// arrays: the kernels' software pipelines read up to 34 pixels past either end
+// of a forest without bounds checks (the values are never used).
+#define LYA_MARGIN 64
+
+// Device-side statistics slots (unsigned long long counters).
+enum { ST_EVALUATED = 0, ST_RECHECK = 1, ST_RUNS = 2, ST_INRANGE = 3, ST_ERROR = 4, ST_N = 8 };
+
+// Forest catalogue on the device.  Per-pixel arrays use a padded CSR: forest f
+// owns pixels pstart[f] .. pstart[f]+len[f]-1, with pstart[f] a multiple of 4 so
+// every forest starts on a 32-byte boundary of the FP64 arrays, and
+// LYA_MARGIN zero pixels before the first and after the last forest.
+struct DevCatalog {
+  int64_t n = 0;          // forests
+  int64_t npix = 0;       // real pixels
+  int64_t npad = 0;       // padded pixel slots
+  int32_t n_slots = 0;
+  int64_t* pstart = nullptr;   // [n]
+  int32_t* len = nullptr;      // [n]
+  uint8_t* sorted = nullptr;   // [n] 1 when dc is non-decreasing
+  int32_t* slot = nullptr;     // [n] owner histogram
+  double* ux = nullptr;        // [n]
+  double* uy = nullptr;
+  double* uz = nullptr;
+  double* ra = nullptr;
+  double* dec = nullptr;
+  long long* name = nullptr;
+  double* omega = nullptr;
+  double* odl2 = nullptr;
+  // FP64 per pixel (padded)
+  double* dc = nullptr;
+  double* w = nullptr;
+  double* dw = nullptr;
+  double* z = nullptr;
+  double* dl = nullptr;
+  // packed FP64 per pixel (padded): (dc, w, dw, z)
+  double4* pix8 = nullptr;
+  // FP32 per pixel (padded): (dc_hi, dc_lo, w, dw) and z
+  float4* pix4 = nullptr;
+  float* z32 = nullptr;
+  bool has_dl = false;
+  bool has_moments = false;
+};
+
+struct WorkQueue {
+  int64_t n_pairs = 0;
+  int32_t* f1 = nullptr;       // [n_pairs] grouped by f1 (non-decreasing)
+  int32_t* f2 = nullptr;       // [n_pairs]
+  double ref_pairs = 0.0;      // sum len1*len2
+};
+
+struct lya_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+
+  bool bins_set = false;
+  double rpmax = 200.0, rtmax = 200.0;
+  int32_t np = 50, nt = 50;
+
+  DevCatalog cat;
+  std::vector<int64_t> h_start;  // host copy of the CSR offsets (unpadded)
+  std::vector<int64_t> h_pstart;
+  std::vector<int32_t> h_slot;
+
+  WorkQueue wq;
+  int cos_variant = 0;
+
+  // correlation outputs: per slot, LYA_NQ quantities as (hi, lo) FP64 pairs,
+  // and pair counts
+  double* hist = nullptr;            // [n_slots][LYA_NQ][2][nb]
+  unsigned long long* counts = nullptr;  // [n_slots][nb]
+  int32_t hist_slots = 0, hist_nb = 0;
+  bool have_result = false;
+
+  unsigned long long* stats = nullptr;   // [ST_N]
+  int64_t* cta_begin = nullptr;          // [max ctas + 1]
+  int32_t cta_cap = 0;
+
+  lya_stats_t last{};
+};
+
+// ------------------------------------------------------------------ errors
+int lya_fail(lya_ctx* ctx, int code, const char* fmt, ...);
+
+#define LYA_CHECK_CUDA(ctx, call)                                                          \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return lya_fail((ctx), LYA_ERR_CUDA, "%s failed: %s", #call,   \
+                                           cudaGetErrorString(e_));                         \
+  } while (0)
+
+template <typename T>
+inline cudaError_t lya_alloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+template <typename T>
+inline void lya_free(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void lya_free_catalog(DevCatalog& c);
+void lya_free_queue(WorkQueue& q);
+
+// ------------------------------------------------------------------ device math
+// cos of the angle between two lines of sight, FP64, in the contraction order
+// nvcc gives the reference's "x1*x2 + y1*y2 + z1*z2" (cuda_kernels.cpp:131);
+// variant selects the order (see the oracle's orc_cos12 for the list).
+__device__ __forceinline__ double lya_cos12(double x1, double y1, double z1, double x2, double y2, double z2,
+                                             int variant) {
+  if (variant == 0) return __fma_rn(z1, z2, __fma_rn(x1, x2, __dmul_rn(y1, y2)));
+  if (variant == 1) return __fma_rn(z1, z2, __fma_rn(y1, y2, __dmul_rn(x1, x2)));
+  return __dadd_rn(__dadd_rn(__dmul_rn(x1, x2), __dmul_rn(y1, y2)), __dmul_rn(z1, z2));
+}
+
+// ------------------------------------------------------------------ launchers
+int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o);
+int lya_build_queue(lya_ctx* ctx, double angmax, double mumin);
+int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w);
+int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out);

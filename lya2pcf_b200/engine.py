@@ -1,0 +1,140 @@
+"""Host-side driver of the native pair-binning library.
+
+:class:`PairEngine` owns one library context on one GPU: it uploads a
+:class:`~lya2pcf_b200.forests.ForestSet`, builds (or receives) the forest-pair
+work queue, runs the histogram kernels and copies results back.  It is the
+layer under the drop-in ``correlation_procedures_pycuda`` module and the
+benchmark.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from . import parameters as P
+
+
+def owner_slots(pix):
+    """Slot index of every forest: pixels numbered in order of first appearance.
+
+    Forests of one pixel must be contiguous (as in a pixel dict).  Returns
+    ``(slot_of_forest int32, slot_pixels int64)``."""
+    pix = np.asarray(pix, dtype=np.int64)
+    if pix.size == 0:
+        return np.zeros(0, dtype=np.int32), np.zeros(0, dtype=np.int64)
+    change = np.ones(pix.size, dtype=bool)
+    change[1:] = pix[1:] != pix[:-1]
+    slot = (np.cumsum(change) - 1).astype(np.int32)
+    slot_pixels = pix[change]
+    if len(np.unique(slot_pixels)) != len(slot_pixels):
+        raise ValueError('forests of one healpix pixel must be contiguous in forest order')
+    return slot, slot_pixels
+
+
+class PairEngine:
+    """One GPU context of the pair-binning library."""
+
+    def __init__(self, device=0, rpmax=P.rpmax, rtmax=P.rtmax, np_=P.numpix_rp, nt=P.numpix_rt):
+        self.lib = N.load()
+        self.ctx = C.c_void_p()
+        N.check(self.lib.lya_ctx_create(int(device), C.byref(self.ctx)))
+        self.np_, self.nt = int(np_), int(nt)
+        self.nb = self.np_ * self.nt
+        self.rpmax, self.rtmax = float(rpmax), float(rtmax)
+        self._check(self.lib.lya_set_bins(self.ctx, self.rpmax, self.rtmax, self.np_, self.nt))
+        self.fs = None
+        self.slot_pixels = None
+        self.n_pairs = 0
+        self._keep = []
+
+    def _check(self, rc):
+        N.check(rc, self.ctx)
+
+    def close(self):
+        if self.ctx:
+            self.lib.lya_ctx_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ upload
+    def upload(self, fs):
+        slot, slot_pixels = owner_slots(fs.pix)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        arrs = dict(start=np.ascontiguousarray(fs.start, dtype=np.int64), dc=f64(fs.dc), w=f64(fs.w),
+                    dw=f64(fs.dw), z=f64(fs.z), dl=f64(fs.dl), ux=f64(fs.ux), uy=f64(fs.uy), uz=f64(fs.uz),
+                    ra=f64(fs.ra), dec=f64(fs.dec), name=np.ascontiguousarray(fs.name, dtype=np.int64),
+                    slot=np.ascontiguousarray(slot, dtype=np.int32), omega=f64(fs.omega), odl2=f64(fs.odl2))
+        p = N.ptr
+        self._check(self.lib.lya_upload_forests(
+            self.ctx, fs.n, p(arrs['start']), p(arrs['dc']), p(arrs['w']), p(arrs['dw']), p(arrs['z']),
+            p(arrs['dl']), p(arrs['ux']), p(arrs['uy']), p(arrs['uz']), p(arrs['ra']), p(arrs['dec']),
+            p(arrs['name']), p(arrs['slot']), int(len(slot_pixels)), p(arrs['omega']), p(arrs['odl2'])))
+        self.fs = fs
+        self.slot_of_forest = slot
+        self.slot_pixels = slot_pixels
+        self.n_pairs = 0
+        return self
+
+    # ------------------------------------------------------------------ work queue
+    def build_pairs(self, angmax):
+        """Neighbour search on the device (``quasar.neighborhood`` for every forest)."""
+        n = C.c_int64(0)
+        self._check(self.lib.lya_build_pairs(self.ctx, float(angmax), float(np.cos(angmax)), C.byref(n)))
+        self.n_pairs = int(n.value)
+        return self.n_pairs
+
+    def set_pairs(self, f1, f2):
+        f1 = np.ascontiguousarray(f1, dtype=np.int32)
+        f2 = np.ascontiguousarray(f2, dtype=np.int32)
+        if f1.shape != f2.shape:
+            raise ValueError('f1 and f2 differ in length')
+        self._check(self.lib.lya_set_pairs(self.ctx, len(f1), N.ptr(f1), N.ptr(f2)))
+        self.n_pairs = len(f1)
+
+    def get_pairs(self):
+        f1 = np.zeros(max(self.n_pairs, 1), dtype=np.int32)
+        f2 = np.zeros(max(self.n_pairs, 1), dtype=np.int32)
+        self._check(self.lib.lya_get_pairs(self.ctx, N.ptr(f1), N.ptr(f2)))
+        return f1[:self.n_pairs], f2[:self.n_pairs]
+
+    # ------------------------------------------------------------------ correlation
+    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0):
+        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), 0)
+        self._check(self.lib.lya_corr_run(self.ctx, C.byref(opts)))
+        return self.stats()
+
+    def histograms(self, slot_first=0, n=None, out=None, counts_out=None):
+        """``(hist[n, 5, nb] float64, counts[n, nb] uint64)`` for slots
+        ``slot_first .. slot_first+n-1`` (W, DW, RP, RT, Z sums; see _native.Q_*)."""
+        nslots = len(self.slot_pixels)
+        n = nslots - slot_first if n is None else int(n)
+        hist = out if out is not None else np.zeros((n, N.NQ, self.nb), dtype=np.float64)
+        cnt = counts_out if counts_out is not None else np.zeros((n, self.nb), dtype=np.uint64)
+        self._check(self.lib.lya_corr_get(self.ctx, int(slot_first), n, N.ptr(hist), N.ptr(cnt)))
+        return hist, cnt
+
+    def adjoint(self, g):
+        """Gradient of sum_b g_b DW_b/W_b w.r.t. dw and w of every pixel (CSR order)."""
+        g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1)
+        if g.size != self.nb:
+            raise ValueError(f'g must have {self.nb} entries')
+        gdw = np.zeros(self.fs.npix_total, dtype=np.float64)
+        gw = np.zeros(self.fs.npix_total, dtype=np.float64)
+        self._check(self.lib.lya_corr_adjoint(self.ctx, N.ptr(g), N.ptr(gdw), N.ptr(gw)))
+        return gdw, gw
+
+    def stats(self):
+        st = N.Stats()
+        self._check(self.lib.lya_stats(self.ctx, C.byref(st)))
+        return st.as_dict()
