@@ -1,0 +1,429 @@
+"""Benchmark of the lya2pcf pair-binning path on B200.
+
+Metric: pixel pairs binned per second.  A pixel pair is one pair (i in f1,
+j in f2) of a neighbouring forest pair as the reference enumerates them
+(``forest_class.quasar.neighborhood``), i.e. the unit of work of the
+reference's ``pair_correlation`` kernel; a step counts sum(len1 * len2) over
+its forest pairs whether or not the kernel needed to evaluate every pair.
+
+One step = the whole job on one catalogue resident in HBM: device neighbour
+search (work queue) + the per-slot histograms (W, DW, counts, RP, RT, Z) in
+one persistent launch.  Workload: the 150,000-forest synthetic catalogue
+(8,000 deg^2, 50x50 bins to 200 Mpc/h).  With N GPUs every rank bins its own
+catalogue of that size (different seed): weak scaling, no data-path
+collective.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'pixel-pairs binned/s: FP32-guarded vs plain FP64 GPU at bit-exact counts'
+UNIT = 'pixel-pairs/s'
+WORKLOAD = ('150,000 synthetic Lyman-alpha forests on 8,000 deg^2 (19/deg^2), lengths U[50,700] clamped to the '
+            '614-pixel log-lambda grid, 50x50 (r_par, r_perp) bins to 200 Mpc/h, float64 inputs')
+GUARD = 1e-4     # Mpc/h guard band of the FP32 kernel
+KERNEL_CODES = {'fp32': 0, 'fp64diag': 1, 'fp64plain': 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--config', type=int, default=1)
+    ap.add_argument('--scale', type=float, default=1.0)
+    ap.add_argument('--kernel', default='fp32', choices=list(KERNEL_CODES))
+    ap.add_argument('--e2e-steps', type=int, default=2)
+    ap.add_argument('--cpu-seconds', type=float, default=15.0, help='target CPU-baseline sample duration')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-compare', action='store_true', help='skip the FP64 comparison sample')
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed plumbing
+class Dist:
+    def __init__(self, want):
+        self.world = int(os.environ.get('WORLD_SIZE', '1'))
+        self.rank = int(os.environ.get('RANK', '0'))
+        self.local = int(os.environ.get('LOCAL_RANK', '0'))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            backend = 'nccl' if self._cuda() else 'gloo'
+            if backend == 'nccl':
+                import torch
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    @staticmethod
+    def _cuda():
+        try:
+            import torch
+            return torch.cuda.is_available()
+        except Exception:
+            return False
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        dev = torch.device('cuda', self.local) if self._cuda() else torch.device('cpu')
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if not self.pg:
+            return v
+        import torch
+        dev = torch.device('cuda', self.local) if self._cuda() else torch.device('cpu')
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    def __init__(self, gpu_index):
+        self.path = tempfile.mktemp(suffix='.csv')
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(gpu_index),
+                 '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+                 'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+                 'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap',
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(',')]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace('.', '', 1).isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace('.', '', 1).isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[k] for r in rows for k in range(4) if 'Active' in r[4 + k] and 'Not' not in r[4 + k]})
+        busy = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)]
+        return {'sm_mhz': statistics.median(busy or sm) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(rows)}
+
+
+# ---------------------------------------------------------------- CPU baseline (oracle port)
+def cpu_baseline(fs, angmax, seconds, seed=5):
+    """Time the CPU restatement of the reference kernel (oracle) on a bounded,
+    seeded sample of owner pixels of the same catalogue, all host cores."""
+    from oracle import oracle as O
+    cores = len(os.sched_getaffinity(0))
+    off, nbr = O.neighbours(fs, angmax, nthreads=cores)
+    f1, f2, sis, pixels = O.items_from_csr(fs, off, nbr)
+    L = fs.lengths
+    slot_pairs = np.array([np.sum(L[f1[sis[s]:sis[s + 1]]] * L[f2[sis[s]:sis[s + 1]]]) for s in range(len(pixels))],
+                          dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(pixels))
+    # calibrate the single-core rate on ~3e8 pixel pairs of one pixel, then take
+    # enough pixels for the target duration on all cores
+    s0 = order[0]
+    it = np.arange(sis[s0], sis[s0 + 1])
+    csum = np.cumsum(L[f1[it]] * L[f2[it]])
+    m = min(int(np.searchsorted(csum, 3e8)) + 1, len(it))
+    t = time.perf_counter()
+    O.corr(fs, f1[it[:m]], f2[it[:m]], np.array([0, m]), nthreads=1)
+    dt = max(time.perf_counter() - t, 1e-3)
+    rate1 = max(float(csum[min(m, len(csum)) - 1]) / dt, 1e7)
+    target = rate1 * cores * seconds
+    chosen, acc = [], 0.0
+    for s in order:
+        chosen.append(s)
+        acc += slot_pairs[s]
+        if acc >= target or len(chosen) >= 4 * cores and acc >= 0.5 * target:
+            break
+    chosen = np.array(sorted(chosen))
+    idx = np.concatenate([np.arange(sis[s], sis[s + 1]) for s in chosen])
+    cnts = np.array([sis[s + 1] - sis[s] for s in chosen])
+    sis_c = np.zeros(len(chosen) + 1, dtype=np.int64)
+    np.cumsum(cnts, out=sis_c[1:])
+    t = time.perf_counter()
+    O.corr(fs, f1[idx], f2[idx], sis_c, nthreads=cores)
+    dt = time.perf_counter() - t
+    pairs = float(np.sum(slot_pairs[chosen]))
+    return {'value': pairs / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+            'sample': f'{len(chosen)} of {len(pixels)} owner pixels (seeded), {pairs:.3e} pixel pairs, '
+                      f'{dt:.1f} s; FP64 every pixel pair like the reference kernel',
+            'seconds': dt, 'pairs': pairs}
+
+
+def build_catalog(config, scale, rank):
+    from lya2pcf_b200 import synthetic
+    seed = synthetic.SEEDS[config] + 1000 * rank
+    fs = synthetic.make(config, scale=scale, seed=seed)
+    return fs, synthetic.angmax_for(fs)
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, dist):
+    fs, angmax = build_catalog(args.config, args.scale, 0)
+    vals = []
+    base = None
+    for k in range(args.warmup + args.steps):
+        b = cpu_baseline(fs, angmax, args.cpu_seconds / 2 if k < args.warmup else args.cpu_seconds, seed=5 + k)
+        if k >= args.warmup:
+            vals.append(b['value'])
+            base = b
+    value = float(np.median(vals))
+    return {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': int(os.environ.get('WORLD_SIZE', args.gpus)),
+            'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * base['seconds'], 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'impl': 'reference',
+            'config': {'workload': WORKLOAD, 'forests': fs.n, 'config': args.config, 'scale': args.scale},
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': base['cores'], 'kind': base['kind'],
+                             'sample': base['sample']},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+
+
+# ---------------------------------------------------------------- B200 arm
+def pinned_copy(a):
+    import torch
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out, t
+
+
+def run_b200(args, dist):
+    import torch
+    from lya2pcf_b200 import _native as N
+    from lya2pcf_b200.engine import PairEngine, owner_slots
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    fs, angmax = build_catalog(args.config, args.scale, dist.rank)
+    kern = KERNEL_CODES[args.kernel]
+    eng = PairEngine(device=dev).upload(fs)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json')))
+    except Exception:
+        pass
+
+    def step():
+        eng.build_pairs(angmax)
+        return eng.run(kernel=kern, guard=GUARD)
+
+    for _ in range(args.warmup):
+        step()
+    st0 = eng.stats()
+    launches0 = st0['launches']
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev) if dist.rank == 0 else None
+    kernel_ms, build_ms = [], []
+    eng.timer_start()
+    for _ in range(args.steps):
+        st = step()
+        kernel_ms.append(st['kernel_ms'])
+        build_ms.append(st['build_ms'])
+    dev_ms = eng.timer_stop()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop() if clocks else None
+    st = eng.stats()
+    launches = st['launches'] - launches0
+    ref_pairs = st['ref_pairs']
+    t_max = dist.max(dev_ms)
+    pairs_all = dist.sum(ref_pairs * args.steps)
+    value = pairs_all / (t_max * 1e-3)
+
+    # ---- e2e through the C ABI with host buffers (pinned), copies inside the region
+    slot, slot_pixels = owner_slots(fs.pix)
+    host = {}
+    keep = []
+    for k, a in dict(start=fs.start.astype(np.int64), dc=fs.dc, w=fs.w, dw=fs.dw, z=fs.z, dl=fs.dl, ux=fs.ux,
+                     uy=fs.uy, uz=fs.uz, ra=fs.ra, dec=fs.dec, name=fs.name.astype(np.int64),
+                     slot=slot.astype(np.int32), omega=fs.omega, odl2=fs.odl2).items():
+        host[k], t = pinned_copy(np.ascontiguousarray(a))
+        keep.append(t)
+    nslot = len(slot_pixels)
+    hist_out, t1 = pinned_copy(np.zeros((nslot, N.NQ, eng.nb), dtype=np.float64))
+    cnt_out, t2 = pinned_copy(np.zeros((nslot, eng.nb), dtype=np.uint64))
+    keep += [t1, t2]
+    h2d = int(sum(a.nbytes for a in host.values()))
+    d2h = int(hist_out.nbytes + cnt_out.nbytes)
+    L = N.load()
+    p = N.ptr
+
+    def e2e_step():
+        N.check(L.lya_upload_forests(eng.ctx, fs.n, p(host['start']), p(host['dc']), p(host['w']), p(host['dw']),
+                                     p(host['z']), p(host['dl']), p(host['ux']), p(host['uy']), p(host['uz']),
+                                     p(host['ra']), p(host['dec']), p(host['name']), p(host['slot']), nslot,
+                                     p(host['omega']), p(host['odl2'])), eng.ctx)
+        eng.build_pairs(angmax)
+        eng.run(kernel=kern, guard=GUARD)
+        N.check(L.lya_corr_get(eng.ctx, 0, nslot, p(hist_out), p(cnt_out)), eng.ctx)
+
+    e2e_step()
+    dist.barrier()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = dist.max(time.perf_counter() - t)
+    e2e_value = dist.sum(ref_pairs * args.e2e_steps) / e2e_s
+
+    out = None
+    if dist.rank == 0:
+        # ---- FP32 vs FP64 on a sample of owner slots: bit-exact counts and pairs/s
+        compare = None
+        if not args.no_compare:
+            compare = fp64_comparison(eng, fs, kern)
+        # ---- roofline of the dominant kernel (the pair kernel)
+        kms = float(np.median(kernel_ms))
+        algo_bytes = st['ref_pixels'] * 24.0          # dc, w, dw (FP64) of both forests per forest pair
+        achieved = algo_bytes / (kms * 1e-3) / 1e9
+        hbm = peaks.get('hbm_gbs')
+        traffic = dram_traffic_per_launch(st['ref_pairs'])
+        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': hbm if hbm else 6650.0, 'unit': 'GB/s',
+                'frac': achieved / (hbm if hbm else 6650.0), 'traffic': traffic,
+                'peak_source': 'measured' if hbm else 'fallback',
+                'kernel': 'k_corr<FP32_GUARDED> (pair kernel)', 'kernel_ms': kms,
+                'algorithmic_bytes_per_launch': algo_bytes,
+                'note': 'not HBM-bound: the forests are re-read from L2; the bound is FP32 issue (see alu)',
+                'alu': alu_roofline(st, kms, clk)}
+        cpu = None if args.no_cpu_baseline else cpu_baseline(fs, angmax, args.cpu_seconds)
+        ms_step = t_max / args.steps
+        out = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': dist.world, 'steps': args.steps,
+               'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+               'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded catalogue, no public data set)',
+               'config': {'workload': WORKLOAD, 'config': args.config, 'scale': args.scale, 'forests': fs.n,
+                          'owner_pixels': nslot, 'forest_pairs': st['n_pairs'],
+                          'ref_pixel_pairs_per_step': ref_pairs, 'kernel': args.kernel, 'guard_mpc_h': GUARD,
+                          'guard_bound_mpc_h': st['guard_bound'], 'l2': 'inputs larger than L2 '
+                          f'({fs.npix_total * 52 / 1e9:.1f} GB resident catalogue)',
+                          'step': 'device neighbour search + histogram run',
+                          'parallelism': f'weak: {dist.world} rank(s), one catalogue each'},
+               'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+                       'path': 'lya_upload_forests + lya_build_pairs + lya_corr_run + lya_corr_get, pinned host'},
+               'gpu_launches': int(launches),
+               'kernel_ms': kms, 'build_ms': float(np.median(build_ms)),
+               'evaluated_pairs_per_step': st['evaluated_pairs'], 'guard_rechecks_per_step': st['guard_rechecks'],
+               'guard_fraction': st['guard_rechecks'] / max(st['evaluated_pairs'], 1.0),
+               'roofline': roof, 'clocks': clk, 'cpu_baseline': cpu, 'fp64_comparison': compare}
+    eng.close()
+    return out
+
+
+def fp64_comparison(eng, fs, kern):
+    """FP32-guarded vs FP64 kernels on the same slots: counts must be equal."""
+    from lya2pcf_b200.engine import owner_slots
+    slot, pixels = owner_slots(fs.pix)
+    nslot = len(pixels)
+    rng = np.random.default_rng(9)
+    s0 = int(rng.integers(0, max(1, nslot - 40)))
+    rngs = (s0, min(nslot, s0 + 40))
+    res = {}
+    counts = {}
+    for name, code in (('fp32_guarded', 0), ('fp64_diagonal', 1), ('fp64_plain', 2)):
+        st = eng.run(kernel=code, guard=GUARD, slots=rngs)
+        st = eng.run(kernel=code, guard=GUARD, slots=rngs)
+        h, c = eng.histograms(rngs[0], rngs[1] - rngs[0])
+        counts[name] = c
+        res[name] = {'pairs_per_s': st['run_ref_pairs'] / (st['kernel_ms'] * 1e-3), 'kernel_ms': st['kernel_ms'],
+                     'W_sum': float(h[:, 0].sum())}
+    res['slots'] = list(rngs)
+    res['ref_pairs'] = st['run_ref_pairs']
+    res['counts_equal_fp32_fp64diag'] = bool(np.array_equal(counts['fp32_guarded'], counts['fp64_diagonal']))
+    res['counts_equal_fp32_fp64plain'] = bool(np.array_equal(counts['fp32_guarded'], counts['fp64_plain']))
+    res['speedup_fp32_vs_fp64plain'] = res['fp32_guarded']['pairs_per_s'] / res['fp64_plain']['pairs_per_s']
+    res['speedup_fp32_vs_fp64diag'] = res['fp32_guarded']['pairs_per_s'] / res['fp64_diagonal']['pairs_per_s']
+    return res
+
+
+def dram_traffic_per_launch(ref_pairs):
+    """DRAM bytes per pair-kernel launch from the committed ncu capture
+    (profiles/k_corr_fp32.json), scaled to this launch's pixel pairs."""
+    try:
+        prof = json.load(open(os.path.join(ROOT, 'profiles', 'k_corr_fp32.json')))
+        return prof['dram_bytes'] / prof['ref_pairs'] * ref_pairs
+    except Exception:
+        return None
+
+
+def alu_roofline(st, kms, clk):
+    """Pair evaluations per second against the FP32 issue bound: the FP32
+    operations one pixel pair needs (the reference's 10 + 7 for the new
+    outputs, SURVEY cost model) at the B200's FP32 rate."""
+    evals = st['evaluated_pairs'] / (kms * 1e-3)
+    sm_mhz = (clk or {}).get('sm_mhz') or 1965.0
+    fp32_lanes = 148 * 128 * sm_mhz * 1e6        # FP32 lane-instructions per second
+    ops = 17.0
+    bound = fp32_lanes / ops
+    return {'pair_evals_per_s': evals, 'fp32_ops_per_pair': ops, 'bound_pair_evals_per_s': bound,
+            'frac': evals / bound, 'sm_mhz_used': sm_mhz}
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        # the reference path is CPU code: rank 0 alone runs it, other ranks exit
+        if int(os.environ.get('RANK', '0')) != 0:
+            return
+        out = run_reference(args, None)
+        print(json.dumps(out), flush=True)
+        return
+    dist = Dist(args.gpus)
+    try:
+        out = run_b200(args, dist)
+        if dist.rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == '__main__':
+    main()

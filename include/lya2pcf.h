@@ -43,9 +43,10 @@ typedef struct lya_ctx lya_ctx;
 typedef struct {
   int32_t kernel;          /* LYA_KERNEL_* */
   double guard;            /* guard half-width around bin edges, Mpc/h (FP32 kernel) */
-  int32_t warps_per_block; /* 0 = autotuned/default */
+  int32_t warps_per_block; /* 0 = default (16) */
   int32_t blocks_per_sm;   /* 0 = default (1) */
-  int32_t use_graph;       /* replay the run through a captured CUDA graph */
+  int32_t slot_begin;      /* restrict the run to pairs whose first forest's */
+  int32_t slot_end;        /* slot is in [slot_begin, slot_end); 0,0 = all    */
 } lya_corr_opts;
 
 typedef struct {
@@ -60,6 +61,10 @@ typedef struct {
   int32_t n_slots;
   int32_t n_forests;
   double guard_bound;      /* proven FP32 error bound, Mpc/h */
+  double run_ms;           /* device time of the last lya_corr_run (all its work) */
+  double run_ref_pairs;    /* reference pair count of the last run's slot range */
+  int64_t launches;        /* kernels of this library launched by the context so far */
+  double ref_pixels;       /* sum over forest pairs of len1+len2 */
 } lya_stats_t;
 
 /* ----------------------------------------------------------------- context */
@@ -115,10 +120,25 @@ int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double* hist, uint
 
 /* Gradient of L = sum_b g[b] * DW_b / W_b (totals over all slots of the last
  * lya_corr_run) with the pair bins held fixed: grad_dw and grad_w per pixel of
- * the catalogue (CSR order).  No reference counterpart. */
-int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w);
+ * the catalogue (CSR order).  g is a host array of np*nt values; grad_dw and
+ * grad_w are host arrays, or device arrays on the context's device when
+ * device_ptrs is 1.  No reference counterpart. */
+int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int32_t device_ptrs);
+
+/* Replace the weights w and weighted deltas dw of every pixel (CSR order, as
+ * uploaded) without re-uploading the catalogue; host arrays, or device arrays
+ * when device_ptrs is 1.  Used between forward evaluations of the adjoint
+ * (fill_dw of forest_class.py:48-68 changes dw when delta or w change). */
+int lya_update_weights(lya_ctx* ctx, const double* w, const double* dw, int32_t device_ptrs);
 
 int lya_stats(lya_ctx* ctx, lya_stats_t* out);
+
+/* Device timer on the context's stream: op 0 records the start event, op 1
+ * records the stop event, waits for it and writes the elapsed milliseconds. */
+int lya_timer(lya_ctx* ctx, int32_t op, double* ms);
+
+/* Block until all work queued on the context's stream has finished. */
+int lya_sync(lya_ctx* ctx);
 
 #ifdef __cplusplus
 }

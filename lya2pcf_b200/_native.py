@@ -35,8 +35,11 @@ SIGNATURES = {
     'lya_get_pairs': ([P, P, P], C.c_int),
     'lya_corr_run': ([P, P], C.c_int),
     'lya_corr_get': ([P, C.c_int32, C.c_int32, P, P], C.c_int),
-    'lya_corr_adjoint': ([P, P, P, P], C.c_int),
+    'lya_corr_adjoint': ([P, P, P, P, C.c_int32], C.c_int),
+    'lya_update_weights': ([P, P, P, C.c_int32], C.c_int),
     'lya_stats': ([P, P], C.c_int),
+    'lya_timer': ([P, C.c_int32, C.POINTER(C.c_double)], C.c_int),
+    'lya_sync': ([P], C.c_int),
 }
 
 
@@ -48,14 +51,15 @@ class LyaError(RuntimeError):
 
 class CorrOpts(C.Structure):
     _fields_ = [('kernel', C.c_int32), ('guard', C.c_double), ('warps_per_block', C.c_int32),
-                ('blocks_per_sm', C.c_int32), ('use_graph', C.c_int32)]
+                ('blocks_per_sm', C.c_int32), ('slot_begin', C.c_int32), ('slot_end', C.c_int32)]
 
 
 class Stats(C.Structure):
     _fields_ = [('ref_pairs', C.c_double), ('evaluated_pairs', C.c_double), ('guard_rechecks', C.c_double),
                 ('runs_flushed', C.c_double), ('in_range_pairs', C.c_double), ('kernel_ms', C.c_double),
                 ('build_ms', C.c_double), ('n_pairs', C.c_int64), ('n_slots', C.c_int32), ('n_forests', C.c_int32),
-                ('guard_bound', C.c_double)]
+                ('guard_bound', C.c_double), ('run_ms', C.c_double), ('run_ref_pairs', C.c_double),
+                ('launches', C.c_int64), ('ref_pixels', C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

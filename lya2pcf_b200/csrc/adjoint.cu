@@ -21,8 +21,6 @@
 
 namespace {
 
-constexpr unsigned FULL = 0xffffffffu;
-
 struct AdjParams {
   const double* __restrict__ dc;
   const double* __restrict__ w;
@@ -135,7 +133,7 @@ __global__ void k_unpad(int64_t n, const int64_t* __restrict__ start, const int6
 
 }  // namespace
 
-int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w) {
+int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int device_ptrs) {
   const int nb = ctx->np * ctx->nt;
   const int64_t n = ctx->cat.n;
   const int64_t npad = ctx->cat.npad, npix = ctx->cat.npix;
@@ -156,6 +154,7 @@ int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* g
   if (e == cudaSuccess) e = cudaMemsetAsync(gw, 0, sizeof(double) * npad, s);
   if (e == cudaSuccess) {
     k_coef<<<(nb + 255) / 256, 256, 0, s>>>(ctx->hist_slots, nb, ctx->hist, d_g, coef);
+    ctx->launches++;
     AdjParams p;
     p.dc = ctx->cat.dc; p.w = ctx->cat.w; p.dw = ctx->cat.dw; p.pstart = ctx->cat.pstart; p.len = ctx->cat.len;
     p.sorted = ctx->cat.sorted; p.ux = ctx->cat.ux; p.uy = ctx->cat.uy; p.uz = ctx->cat.uz;
@@ -165,16 +164,26 @@ int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* g
     p.coef = coef; p.g_dw = gdw; p.g_w = gw;
     const size_t smem = sizeof(double) * 2 * nb;
     e = cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess && p.n_items > 0) k_adjoint<<<ctx->num_sms * 4, 256, smem, s>>>(p);
+    if (e == cudaSuccess && p.n_items > 0) {
+      k_adjoint<<<ctx->num_sms * 4, 256, smem, s>>>(p);
+      ctx->launches++;
+    }
     if (e == cudaSuccess) e = cudaGetLastError();
   }
   if (e == cudaSuccess && n > 0) {
     const int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
-    k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gdw, out);
-    if (grad_dw) e = cudaMemcpyAsync(grad_dw, out, sizeof(double) * npix, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gw, out);
-    if (e == cudaSuccess && grad_w) e = cudaMemcpyAsync(grad_w, out, sizeof(double) * npix, cudaMemcpyDeviceToHost, s);
+    if (device_ptrs) {
+      if (grad_dw) { k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gdw, grad_dw); ctx->launches++; }
+      if (grad_w) { k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gw, grad_w); ctx->launches++; }
+    } else {
+      k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gdw, out);
+      ctx->launches++;
+      if (grad_dw) e = cudaMemcpyAsync(grad_dw, out, sizeof(double) * npix, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gw, out);
+      ctx->launches++;
+      if (e == cudaSuccess && grad_w) e = cudaMemcpyAsync(grad_w, out, sizeof(double) * npix, cudaMemcpyDeviceToHost, s);
+    }
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cleanup();
@@ -182,10 +191,10 @@ int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* g
   return LYA_OK;
 }
 
-extern "C" int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w) {
+extern "C" int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int32_t device_ptrs) {
   if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_corr_adjoint: ctx is NULL");
   if (!g) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_adjoint: g is NULL");
   if (!ctx->have_result) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_adjoint: run lya_corr_run first");
   LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
-  return lya_adjoint_launch(ctx, g, grad_dw, grad_w);
+  return lya_adjoint_launch(ctx, g, grad_dw, grad_w, device_ptrs);
 }

@@ -69,6 +69,10 @@ extern "C" int lya_ctx_create(int device, lya_ctx** out) {
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
     if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
     if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaEventCreate(&ctx->ev2)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaEventCreate(&ctx->ev3)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaEventCreate(&ctx->tev0)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
+    if ((e = cudaEventCreate(&ctx->tev1)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
     if ((e = lya_alloc(&ctx->stats, ST_N)) != cudaSuccess) { rc = LYA_ERR_ALLOC; break; }
   } while (0);
   if (rc != LYA_OK) {
@@ -89,6 +93,10 @@ extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
   lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->ev2) cudaEventDestroy(ctx->ev2);
+  if (ctx->ev3) cudaEventDestroy(ctx->ev3);
+  if (ctx->tev0) cudaEventDestroy(ctx->tev0);
+  if (ctx->tev1) cudaEventDestroy(ctx->tev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return LYA_OK;
@@ -232,6 +240,7 @@ extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start,
     int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
     k_pack<<<blocks, 128, 0, s>>>(n, t_start, c.pstart, t_dc, t_w, t_dw, t_z, t_dl, c.dc, c.w, c.dw, c.z, c.dl,
                                   c.pix8, c.pix4, c.z32, c.len, c.sorted);
+    ctx->launches++;
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -240,6 +249,60 @@ extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start,
     lya_free_catalog(ctx->cat);
     return lya_fail(ctx, LYA_ERR_CUDA, "lya_upload_forests: %s", cudaGetErrorString(e));
   }
+  return LYA_OK;
+}
+
+// ------------------------------------------------------------------ weights update
+__global__ void k_repack_weights(int64_t n, const int64_t* __restrict__ start, const int64_t* __restrict__ pstart,
+                                 const double* __restrict__ w, const double* __restrict__ dw,
+                                 double* __restrict__ o_w, double* __restrict__ o_dw, double4* __restrict__ o_pix8,
+                                 float4* __restrict__ o_pix4) {
+  for (int64_t f = blockIdx.x; f < n; f += gridDim.x) {
+    const int64_t s = start[f], L = start[f + 1] - s, d = pstart[f];
+    for (int64_t k = threadIdx.x; k < L; k += blockDim.x) {
+      const double wv = w[s + k], dv = dw[s + k];
+      o_w[d + k] = wv;
+      o_dw[d + k] = dv;
+      o_pix8[d + k].y = wv;
+      o_pix8[d + k].z = dv;
+      o_pix4[d + k].z = __double2float_rn(wv);
+      o_pix4[d + k].w = __double2float_rn(dv);
+    }
+  }
+}
+
+extern "C" int lya_update_weights(lya_ctx* ctx, const double* w, const double* dw, int32_t device_ptrs) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_update_weights: ctx is NULL");
+  if (ctx->cat.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_update_weights: no forests uploaded");
+  const int64_t npix = ctx->cat.npix, n = ctx->cat.n;
+  if (npix > 0 && (!w || !dw)) return lya_fail(ctx, LYA_ERR_ARG, "lya_update_weights: NULL array");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  double *tw = nullptr, *tdw = nullptr;
+  int64_t* ts = nullptr;
+  cudaError_t e = lya_alloc(&ts, n + 1);
+  if (e == cudaSuccess && !device_ptrs) e = lya_alloc(&tw, npix);
+  if (e == cudaSuccess && !device_ptrs) e = lya_alloc(&tdw, npix);
+  if (e != cudaSuccess) {
+    lya_free(ts); lya_free(tw); lya_free(tdw);
+    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_update_weights: allocation failed");
+  }
+  const double* sw = device_ptrs ? w : tw;
+  const double* sdw = device_ptrs ? dw : tdw;
+  e = cudaMemcpyAsync(ts, ctx->h_start.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !device_ptrs) e = cudaMemcpyAsync(tw, w, sizeof(double) * npix, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !device_ptrs) e = cudaMemcpyAsync(tdw, dw, sizeof(double) * npix, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    const int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
+    k_repack_weights<<<blocks, 128, 0, s>>>(n, ts, ctx->cat.pstart, sw, sdw, ctx->cat.w, ctx->cat.dw, ctx->cat.pix8,
+                                            ctx->cat.pix4);
+    ctx->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  lya_free(ts); lya_free(tw); lya_free(tdw);
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_update_weights: %s", cudaGetErrorString(e));
+  ctx->have_result = false;
   return LYA_OK;
 }
 
@@ -265,7 +328,7 @@ extern "C" int lya_set_pairs(lya_ctx* ctx, int64_t n_pairs, const int32_t* f1, c
     lya_free_queue(q);
     return lya_fail(ctx, LYA_ERR_ALLOC, "lya_set_pairs: device allocation failed");
   }
-  double ref = 0.0;
+  double ref = 0.0, refpix = 0.0;
   for (int64_t k = 0; k < n_pairs; ++k) {
     if (f1[k] < 0 || f1[k] >= ctx->cat.n || f2[k] < 0 || f2[k] >= ctx->cat.n) {
       lya_free_queue(q);
@@ -276,10 +339,14 @@ extern "C" int lya_set_pairs(lya_ctx* ctx, int64_t n_pairs, const int32_t* f1, c
       lya_free_queue(q);
       return lya_fail(ctx, LYA_ERR_ARG, "lya_set_pairs: f1 must be non-decreasing (pair %lld)", (long long)k);
     }
-    ref += (double)(ctx->h_start[f1[k] + 1] - ctx->h_start[f1[k]]) * (double)(ctx->h_start[f2[k] + 1] - ctx->h_start[f2[k]]);
+    const double l1 = (double)(ctx->h_start[f1[k] + 1] - ctx->h_start[f1[k]]);
+    const double l2 = (double)(ctx->h_start[f2[k] + 1] - ctx->h_start[f2[k]]);
+    ref += l1 * l2;
+    refpix += l1 + l2;
   }
   q.n_pairs = n_pairs;
   q.ref_pairs = ref;
+  q.ref_pixels = refpix;
   LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(q.f1, f1, sizeof(int32_t) * n_pairs, cudaMemcpyHostToDevice, ctx->stream));
   LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(q.f2, f2, sizeof(int32_t) * n_pairs, cudaMemcpyHostToDevice, ctx->stream));
   LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -322,6 +389,7 @@ extern "C" int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double*
     const double* src = ctx->hist + (size_t)slot_first * LYA_NQ * 2 * nb;
     int blocks = (int)std::min<int64_t>(((int64_t)n * LYA_NQ * nb + 255) / 256, (int64_t)ctx->num_sms * 8);
     k_combine<<<blocks, 256, 0, ctx->stream>>>(n, nb, src, tmp);
+    ctx->launches++;
     e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(hist, tmp, sizeof(double) * (size_t)n * LYA_NQ * nb, cudaMemcpyDeviceToHost, ctx->stream);
@@ -338,11 +406,36 @@ extern "C" int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double*
   return LYA_OK;
 }
 
+extern "C" int lya_timer(lya_ctx* ctx, int32_t op, double* ms) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_timer: ctx is NULL");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (op == 0) {
+    LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->tev0, ctx->stream));
+    return LYA_OK;
+  }
+  if (op != 1 || !ms) return lya_fail(ctx, LYA_ERR_ARG, "lya_timer: op must be 0 or 1 (with ms)");
+  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->tev1, ctx->stream));
+  LYA_CHECK_CUDA(ctx, cudaEventSynchronize(ctx->tev1));
+  float f = 0.f;
+  LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&f, ctx->tev0, ctx->tev1));
+  *ms = f;
+  return LYA_OK;
+}
+
+extern "C" int lya_sync(lya_ctx* ctx) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_sync: ctx is NULL");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return LYA_OK;
+}
+
 extern "C" int lya_stats(lya_ctx* ctx, lya_stats_t* out) {
   if (!ctx || !out) return lya_fail(ctx, LYA_ERR_ARG, "lya_stats: NULL argument");
   *out = ctx->last;
+  out->launches = ctx->launches;
   out->n_pairs = ctx->wq.n_pairs;
   out->ref_pairs = ctx->wq.ref_pairs;
+  out->ref_pixels = ctx->wq.ref_pixels;
   out->n_slots = ctx->cat.n_slots;
   out->n_forests = (int32_t)ctx->cat.n;
   return LYA_OK;

@@ -587,17 +587,36 @@ cudaError_t launch_corr(const CorrParams& p, int nctas, int nb, cudaStream_t s) 
 __global__ void k_item_cost(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ f2,
                             const int32_t* __restrict__ len, long long* __restrict__ cost) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-    cost[k] = (long long)len[f1[k]] * (long long)len[f2[k]] + 64;   // + fixed per-pair overhead
+    cost[k] = (long long)len[f1[k]] * (long long)len[f2[k]];
 }
 
-__global__ void k_cta_bounds(int nctas, int64_t n, const long long* __restrict__ prefix, int64_t* __restrict__ out) {
+// first item k in [lo, hi) whose first forest's slot is >= s (items are grouped
+// by first forest, slots non-decreasing in forest order)
+__device__ int64_t first_item_of_slot(const int32_t* __restrict__ f1, const int32_t* __restrict__ slot, int64_t lo,
+                                      int64_t hi, int s) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (slot[f1[mid]] < s) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// CTA b takes items [out[b], out[b+1]): equal shares of the reference pair
+// count inside the item range of slots [slot_begin, slot_end).
+__global__ void k_cta_bounds(int nctas, int64_t n, const long long* __restrict__ prefix,
+                             const int32_t* __restrict__ f1, const int32_t* __restrict__ slot, int slot_begin,
+                             int slot_end, int64_t* __restrict__ out, double* __restrict__ range_pairs) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b > nctas) return;
-  if (b == 0) { out[0] = 0; return; }
-  if (b == nctas || n == 0) { out[b] = n; return; }
-  const double total = (double)prefix[n - 1];
-  const long long target = (long long)(total * ((double)b / nctas));
-  int64_t lo = 0, hi = n;   // first k with prefix[k] > target
+  const bool all = slot_begin == 0 && slot_end == 0;
+  const int64_t it_lo = all ? 0 : first_item_of_slot(f1, slot, 0, n, slot_begin);
+  const int64_t it_hi = all ? n : first_item_of_slot(f1, slot, it_lo, n, slot_end);
+  const long long base = it_lo > 0 ? prefix[it_lo - 1] : 0;
+  const long long total = it_hi > it_lo ? prefix[it_hi - 1] - base : 0;
+  if (b == 0) { out[0] = it_lo; *range_pairs = (double)total; return; }
+  if (b == nctas) { out[b] = it_hi; return; }
+  const long long target = base + (long long)((double)total * ((double)b / nctas));
+  int64_t lo = it_lo, hi = it_hi;   // first k with prefix[k] > target
   while (lo < hi) {
     const int64_t mid = (lo + hi) >> 1;
     if (prefix[mid] > target) hi = mid; else lo = mid + 1;
@@ -607,7 +626,8 @@ __global__ void k_cta_bounds(int nctas, int64_t n, const long long* __restrict__
 
 }  // namespace
 
-int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out) {
+int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out, int slot_begin, int slot_end,
+                           double* d_range_pairs) {
   const int64_t n = ctx->wq.n_pairs;
   long long* cost = nullptr;
   cudaError_t e = lya_alloc(&cost, (size_t)std::max<int64_t>(n, 1));
@@ -615,14 +635,15 @@ int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out) {
   if (n > 0) {
     const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 16);
     k_item_cost<<<blocks, 256, 0, ctx->stream>>>(n, ctx->wq.f1, ctx->wq.f2, ctx->cat.len, cost);
+    ctx->launches++;
     thrust::inclusive_scan(thrust::cuda::par.on(ctx->stream), cost, cost + n, cost);
   }
-  k_cta_bounds<<<(nctas + 1 + 127) / 128, 128, 0, ctx->stream>>>(nctas, n, cost, d_out);
+  k_cta_bounds<<<(nctas + 1 + 127) / 128, 128, 0, ctx->stream>>>(nctas, n, cost, ctx->wq.f1, ctx->cat.slot, slot_begin,
+                                                                 slot_end, d_out, d_range_pairs);
+  ctx->launches++;
   e = cudaGetLastError();
-  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
-  lya_free(cost);
-  if (e != cudaSuccess || e2 != cudaSuccess)
-    return lya_fail(ctx, LYA_ERR_CUDA, "cta ranges: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  lya_free(cost);   // cudaFree waits for the queued work
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "cta ranges: %s", cudaGetErrorString(e));
   return LYA_OK;
 }
 
@@ -665,19 +686,22 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
     }
     ctx->hist_slots = nslots; ctx->hist_nb = nb;
   }
+  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev2, s));
   LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->hist, 0, sizeof(double) * (size_t)nslots * LYA_NQ * 2 * nb, s));
   LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->counts, 0, sizeof(unsigned long long) * (size_t)nslots * nb, s));
   LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->stats, 0, sizeof(unsigned long long) * ST_N, s));
 
-  const int warps = o->warps_per_block == 32 ? 32 : 16;
+  const int warps = 16;
   const int nctas = ctx->num_sms * std::max(1, o->blocks_per_sm);
-  if (ctx->cta_cap < nctas + 1) {
+  if (ctx->cta_cap < nctas + 2) {
     lya_free(ctx->cta_begin);
-    if (lya_alloc(&ctx->cta_begin, (size_t)nctas + 1) != cudaSuccess)
+    if (lya_alloc(&ctx->cta_begin, (size_t)nctas + 2) != cudaSuccess)
       return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_run: allocation failed");
-    ctx->cta_cap = nctas + 1;
+    ctx->cta_cap = nctas + 2;
   }
-  int rc = lya_prepare_cta_ranges(ctx, nctas, ctx->cta_begin);
+  // the slot of the range's reference pair count shares the cta_begin buffer
+  double* d_range_pairs = reinterpret_cast<double*>(ctx->cta_begin + nctas + 1);
+  int rc = lya_prepare_cta_ranges(ctx, nctas, ctx->cta_begin, o->slot_begin, o->slot_end, d_range_pairs);
   if (rc != LYA_OK) return rc;
 
   CorrParams p;
@@ -706,13 +730,20 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
   else
     e = launch_corr<LYA_KERNEL_FP64_PLAIN, 16>(p, nctas, nb, s);
   if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run launch: %s", cudaGetErrorString(e));
+  ctx->launches++;
   LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev3, s));
   unsigned long long hst[ST_N];
+  double range_pairs = 0.0;
   LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(hst, ctx->stats, sizeof(hst), cudaMemcpyDeviceToHost, s));
+  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(&range_pairs, d_range_pairs, sizeof(double), cudaMemcpyDeviceToHost, s));
   LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-  float ms = 0.f;
+  float ms = 0.f, ms_all = 0.f;
   LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms_all, ctx->ev2, ctx->ev3));
   ctx->last.kernel_ms = ms;
+  ctx->last.run_ms = ms_all;
+  ctx->last.run_ref_pairs = range_pairs;
   ctx->last.evaluated_pairs = (double)hst[ST_EVALUATED];
   ctx->last.guard_rechecks = (double)hst[ST_RECHECK];
   ctx->last.runs_flushed = (double)hst[ST_RUNS];
@@ -731,6 +762,9 @@ extern "C" int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts) {
   if (o.blocks_per_sm < 0 || o.blocks_per_sm > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: blocks_per_sm must be 0 or 1");
   if (o.warps_per_block != 0 && o.warps_per_block != 16)
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: warps_per_block must be 0 or 16");
+  if (o.slot_begin < 0 || o.slot_end < o.slot_begin || o.slot_end > ctx->cat.n_slots)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: slot range [%d,%d) outside [0,%d]", o.slot_begin, o.slot_end,
+                    ctx->cat.n_slots);
   if (!ctx->bins_set) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_run: call lya_set_bins first");
   if (ctx->cat.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_run: no forests uploaded");
   LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -62,13 +62,17 @@ struct WorkQueue {
   int32_t* f1 = nullptr;       // [n_pairs] grouped by f1 (non-decreasing)
   int32_t* f2 = nullptr;       // [n_pairs]
   double ref_pairs = 0.0;      // sum len1*len2
+  double ref_pixels = 0.0;     // sum len1+len2
 };
 
 struct lya_ctx {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // kernel timing
+  cudaEvent_t ev2 = nullptr, ev3 = nullptr;   // whole-call timing
+  cudaEvent_t tev0 = nullptr, tev1 = nullptr; // lya_timer
+  int64_t launches = 0;
   std::string err;
 
   bool bins_set = false;
@@ -137,5 +141,6 @@ __device__ __forceinline__ double lya_cos12(double x1, double y1, double z1, dou
 // ------------------------------------------------------------------ launchers
 int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o);
 int lya_build_queue(lya_ctx* ctx, double angmax, double mumin);
-int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w);
-int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out);
+int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int device_ptrs);
+int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out, int slot_begin, int slot_end,
+                           double* d_range_pairs);

@@ -151,13 +151,23 @@ __global__ void k_neighbours(const NbrParams p) {
   }
 }
 
+// out[0] += sum len1*len2 (reference pixel pairs), out[1] += sum len1+len2
 __global__ void k_pair_cost(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ f2,
                             const int32_t* __restrict__ len, double* __restrict__ out) {
-  double acc = 0.0;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-    acc += (double)len[f1[k]] * (double)len[f2[k]];
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+  double acc = 0.0, pix = 0.0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const double l1 = (double)len[f1[k]], l2 = (double)len[f2[k]];
+    acc += l1 * l2;
+    pix += l1 + l2;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc += __shfl_xor_sync(FULL, acc, o);
+    pix += __shfl_xor_sync(FULL, pix, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, acc);
+    atomicAdd(out + 1, pix);
+  }
 }
 
 }  // namespace
@@ -181,7 +191,7 @@ int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
   if (e == cudaSuccess) e = lya_alloc(&counts, n + 1);
   if (e == cudaSuccess) e = lya_alloc(&offsets, n + 1);
   if (e == cudaSuccess) e = lya_alloc(&flag, 1);
-  if (e == cudaSuccess) e = lya_alloc(&tot, 1);
+  if (e == cudaSuccess) e = lya_alloc(&tot, 2);
   auto cleanup = [&]() {
     lya_free(band); lya_free(sidx); lya_free(sra); lya_free(bstart); lya_free(counts); lya_free(offsets);
     lya_free(flag); lya_free(tot);
@@ -192,10 +202,11 @@ int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
   }
   LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
   cudaMemsetAsync(flag, 0, sizeof(int), s);
-  cudaMemsetAsync(tot, 0, sizeof(double), s);
+  cudaMemsetAsync(tot, 0, 2 * sizeof(double), s);
   cudaMemsetAsync(counts, 0, sizeof(long long) * (n + 1), s);
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
   k_bands<<<blocks, 256, 0, s>>>(n, ctx->cat.ra, ctx->cat.dec, h, nband, band, sra, sidx, flag);
+  ctx->launches++;
   // order by (band, ra): stable sort by ra, then stable sort by band
   thrust::stable_sort_by_key(pol, sra, sra + n, thrust::make_zip_iterator(thrust::make_tuple(sidx, band)));
   thrust::stable_sort_by_key(pol, band, band + n, thrust::make_zip_iterator(thrust::make_tuple(sidx, sra)));
@@ -209,6 +220,7 @@ int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
   p.of1 = nullptr; p.of2 = nullptr;
   const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, (int64_t)ctx->num_sms * 32));
   k_neighbours<false><<<nblk, 256, 0, s>>>(p);
+  ctx->launches++;
   thrust::exclusive_scan(pol, counts, counts + n + 1, offsets);
   long long npairs = 0;
   e = cudaMemcpyAsync(&npairs, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, s);
@@ -227,14 +239,16 @@ int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
   }
   p.of1 = ctx->wq.f1; p.of2 = ctx->wq.f2;
   k_neighbours<true><<<nblk, 256, 0, s>>>(p);
+  ctx->launches++;
   if (npairs > 0) {
     const int cb = (int)std::min<int64_t>((npairs + 255) / 256, (int64_t)ctx->num_sms * 8);
     k_pair_cost<<<cb, 256, 0, s>>>(npairs, ctx->wq.f1, ctx->wq.f2, ctx->cat.len, tot);
+    ctx->launches++;
   }
-  double ref = 0.0;
+  double ref[2] = {0.0, 0.0};
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&ref, tot, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ref, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   float ms = 0.f;
   if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -244,7 +258,8 @@ int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
     return lya_fail(ctx, LYA_ERR_CUDA, "lya_build_pairs: %s", cudaGetErrorString(e));
   }
   ctx->wq.n_pairs = npairs;
-  ctx->wq.ref_pairs = ref;
+  ctx->wq.ref_pairs = ref[0];
+  ctx->wq.ref_pixels = ref[1];
   ctx->last.build_ms = ms;
   return LYA_OK;
 }

@@ -109,10 +109,26 @@ class PairEngine:
         return f1[:self.n_pairs], f2[:self.n_pairs]
 
     # ------------------------------------------------------------------ correlation
-    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0):
-        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), 0)
+    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0, slots=None):
+        """Histograms of the work queue (restricted to owner slots
+        ``range(*slots)`` when given).  Returns :meth:`stats`."""
+        s0, s1 = (0, 0) if slots is None else (int(slots[0]), int(slots[1]))
+        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), s0, s1)
         self._check(self.lib.lya_corr_run(self.ctx, C.byref(opts)))
         return self.stats()
+
+    def timer_start(self):
+        """Record a start event on the library's stream."""
+        self._check(self.lib.lya_timer(self.ctx, 0, None))
+
+    def timer_stop(self):
+        """Record a stop event, wait for it; device milliseconds since timer_start."""
+        ms = C.c_double(0.0)
+        self._check(self.lib.lya_timer(self.ctx, 1, C.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        self._check(self.lib.lya_sync(self.ctx))
 
     def histograms(self, slot_first=0, n=None, out=None, counts_out=None):
         """``(hist[n, 5, nb] float64, counts[n, nb] uint64)`` for slots
@@ -124,15 +140,32 @@ class PairEngine:
         self._check(self.lib.lya_corr_get(self.ctx, int(slot_first), n, N.ptr(hist), N.ptr(cnt)))
         return hist, cnt
 
-    def adjoint(self, g):
-        """Gradient of sum_b g_b DW_b/W_b w.r.t. dw and w of every pixel (CSR order)."""
+    def adjoint(self, g, out_dw=None, out_w=None):
+        """Gradient of sum_b g_b DW_b/W_b w.r.t. dw and w of every pixel (CSR
+        order), bins held fixed.  ``out_dw``/``out_w`` may be CUDA torch tensors
+        (float64, contiguous, on this context's device) to receive the result on
+        the device; otherwise numpy arrays are returned."""
         g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1)
         if g.size != self.nb:
             raise ValueError(f'g must have {self.nb} entries')
+        if out_dw is not None:
+            self._check(self.lib.lya_corr_adjoint(self.ctx, N.ptr(g), C.c_void_p(out_dw.data_ptr()),
+                                                  C.c_void_p(out_w.data_ptr()), 1))
+            return out_dw, out_w
         gdw = np.zeros(self.fs.npix_total, dtype=np.float64)
         gw = np.zeros(self.fs.npix_total, dtype=np.float64)
-        self._check(self.lib.lya_corr_adjoint(self.ctx, N.ptr(g), N.ptr(gdw), N.ptr(gw)))
+        self._check(self.lib.lya_corr_adjoint(self.ctx, N.ptr(g), N.ptr(gdw), N.ptr(gw), 0))
         return gdw, gw
+
+    def update_weights(self, w, dw):
+        """Replace w and dw of every pixel (numpy arrays, or CUDA float64 torch
+        tensors on this context's device)."""
+        if hasattr(w, 'data_ptr'):
+            self._check(self.lib.lya_update_weights(self.ctx, C.c_void_p(w.data_ptr()), C.c_void_p(dw.data_ptr()), 1))
+        else:
+            w = np.ascontiguousarray(w, dtype=np.float64)
+            dw = np.ascontiguousarray(dw, dtype=np.float64)
+            self._check(self.lib.lya_update_weights(self.ctx, N.ptr(w), N.ptr(dw), 0))
 
     def stats(self):
         st = N.Stats()

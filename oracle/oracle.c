@@ -57,6 +57,11 @@ enum { ORC_GPU_FORMULA = 0, ORC_CPU_FORMULA = 1 };
  *   0: fma(z1,z2, fma(x1,x2, y1*y2))
  *   1: fma(z1,z2, fma(y1,y2, x1*x2))
  *   2: ((x1*x2) + (y1*y2)) + (z1*z2)   (no contraction)                      */
+/* cos12 clamped to [-1, 1]: for coincident lines of sight rounding can give
+ * 1 + ulp, where the reference takes the square root of a negative number
+ * (cuda_kernels.cpp:132-134); the clamp gives the geometric answer rt = 0. */
+static double cos12_clamped(double x1, double y1, double z1, double x2, double y2, double z2, int variant);
+
 double orc_cos12(double x1, double y1, double z1, double x2, double y2, double z2, int variant) {
   switch (variant) {
     case 0: return fma(z1, z2, fma(x1, x2, y1 * y2));
@@ -66,6 +71,11 @@ double orc_cos12(double x1, double y1, double z1, double x2, double y2, double z
       return (a + b) + c;
     }
   }
+}
+
+static double cos12_clamped(double x1, double y1, double z1, double x2, double y2, double z2, int variant) {
+  double c = orc_cos12(x1, y1, z1, x2, y2, z2, variant);
+  return c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
 }
 
 /* ------------------------------------------------------------------ inputs */
@@ -278,7 +288,7 @@ static void corr_pair(const corr_ctx* c, int64_t a, int64_t b, double* h, uint64
   int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
   double chh, shh;
   if (c->mode == ORC_GPU_FORMULA) {
-    double cos12 = orc_cos12(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], c->cos_variant);
+    double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], c->cos_variant);
     chh = sqrt(0.5 * (1. + cos12));
     shh = sqrt(0.5 * (1. - cos12));
   } else {
@@ -391,7 +401,7 @@ int orc_adjoint(const orc_forests* F, int64_t nitem, const int32_t* f1, const in
     int64_t a = f1[it], b = f2[it];
     int64_t s1 = F->start[a], l1 = F->start[a + 1] - s1;
     int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
-    double cos12 = orc_cos12(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
+    double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
     double chh = sqrt(0.5 * (1. + cos12)), shh = sqrt(0.5 * (1. - cos12));
     for (int64_t i = 0; i < l1; ++i) {
       double d1 = F->dc[s1 + i];
@@ -442,7 +452,7 @@ int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const
     int64_t a = f1[it], b = f2[it];
     int64_t s1 = F->start[a], l1 = F->start[a + 1] - s1;
     int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
-    double cos12 = orc_cos12(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
+    double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
     double chh = sqrt(0.5 * (1. + cos12)), shh = sqrt(0.5 * (1. - cos12));
     double om1 = F->omega[a], om2 = F->omega[b], o21 = F->odl2[a], o22 = F->odl2[b];
     memset(e12, 0, sizeof(double) * (size_t)nb * (size_t)l1);

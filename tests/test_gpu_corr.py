@@ -1,0 +1,159 @@
+"""GPU parity of the pair-histogram kernels against the CPU oracle.
+
+Counts are compared bit for bit; floating-point sums within the tolerances
+stated per test (FP32 kernel: 1e-6 relative, normwise for DW against
+sum |dw1 dw2|; FP64 kernels: 1e-12)."""
+import numpy as np
+import pytest
+
+import edge_cases as E
+from lya2pcf_b200 import _native as N
+from lya2pcf_b200 import synthetic
+from lya2pcf_b200.engine import PairEngine
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = [N.KERNEL_FP32_GUARDED, N.KERNEL_FP64_DIAGONAL, N.KERNEL_FP64_PLAIN]
+TOL = {N.KERNEL_FP32_GUARDED: 1e-6, N.KERNEL_FP64_DIAGONAL: 1e-12, N.KERNEL_FP64_PLAIN: 1e-12}
+
+
+def check_hist(h, c, ho, co, kern, label=''):
+    assert np.array_equal(c, co), f'{label}: pair counts differ ({int(np.abs(c.astype(np.int64) - co.astype(np.int64)).sum())} pairs)'
+    tol = TOL[kern]
+    W, Wo = h[:, N.Q_W], ho[:, O.Q_W]
+    assert np.all(np.abs(W - Wo) <= tol * np.abs(Wo) + 1e-300), f'{label}: W'
+    # DW has random signs: compare against its condition scale sum |dw1 dw2|
+    assert np.all(np.abs(h[:, N.Q_DW] - ho[:, O.Q_DW]) <= tol * ho[:, O.Q_DWABS] + 1e-300), f'{label}: DW'
+    for q, qo in ((N.Q_RP, O.Q_RP), (N.Q_RT, O.Q_RT), (N.Q_Z, O.Q_Z)):
+        assert np.all(np.abs(h[:, q] - ho[:, qo]) <= tol * np.abs(ho[:, qo]) + 1e-9 * tol), f'{label}: q{q}'
+
+
+@pytest.fixture(scope='module')
+def cfg0():
+    fs = synthetic.make(0)
+    am = synthetic.angmax_for(fs)
+    eng = PairEngine().upload(fs)
+    eng.build_pairs(am)
+    off, nbr = O.neighbours(fs, am)
+    f1, f2, sis, pixels = O.items_from_csr(fs, off, nbr)
+    yield fs, am, eng, (off, nbr), (f1, f2, sis, pixels)
+    eng.close()
+
+
+def test_device_neighbours_equal_oracle(cfg0):
+    fs, am, eng, (off, nbr), _ = cfg0
+    d1, d2 = eng.get_pairs()
+    assert len(d1) == off[-1]
+    o1 = np.repeat(np.arange(fs.n), np.diff(off))
+    assert set(zip(d1.tolist(), d2.tolist())) == set(zip(o1.tolist(), nbr.tolist()))
+    assert np.all(np.diff(d1) >= 0)          # grouped by first forest
+    st = eng.stats()
+    assert st['ref_pairs'] == float(np.sum(fs.lengths[o1] * fs.lengths[nbr]))
+
+
+@pytest.mark.parametrize('kern', KERNELS)
+def test_config0_slots_match_oracle(cfg0, kern):
+    fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
+    ns = 4
+    ho, co = O.corr(fs, f1[:sis[ns]], f2[:sis[ns]], sis[:ns + 1])
+    eng.run(kernel=kern)
+    h, c = eng.histograms(0, ns)
+    check_hist(h, c, ho, co, kern, f'kernel {kern}')
+
+
+def test_slot_restricted_run(cfg0):
+    fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
+    st = eng.run(kernel=N.KERNEL_FP32_GUARDED, slots=(3, 5))
+    h, c = eng.histograms()
+    assert c[:3].sum() == 0 and c[5:].sum() == 0 and c[3:5].sum() > 0
+    ho, co = O.corr(fs, f1[sis[3]:sis[5]], f2[sis[3]:sis[5]], sis[3:6] - sis[3])
+    assert np.array_equal(c[3:5], co)
+    assert st['run_ref_pairs'] == float(np.sum(fs.lengths[f1[sis[3]:sis[5]]] * fs.lengths[f2[sis[3]:sis[5]]]))
+
+
+def test_fp32_counts_equal_fp64_all_slots(cfg0):
+    fs, am, eng, _, _ = cfg0
+    eng.run(kernel=N.KERNEL_FP32_GUARDED)
+    h32, c32 = eng.histograms()
+    eng.run(kernel=N.KERNEL_FP64_DIAGONAL)
+    h64, c64 = eng.histograms()
+    assert np.array_equal(c32, c64)
+    np.testing.assert_allclose(h32[:, N.Q_W], h64[:, N.Q_W], rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize('kern', KERNELS)
+def test_edge_catalog(kern):
+    fs = E.edge_catalog()
+    am = 0.05
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.build_pairs(am)
+        off, nbr = O.neighbours(fs, am)
+        f1, f2, sis, pixels = O.items_from_csr(fs, off, nbr)
+        d1, d2 = eng.get_pairs()
+        assert set(zip(d1.tolist(), d2.tolist())) == set(zip(f1.tolist(), f2.tolist()))
+        ho, co = O.corr(fs, f1, f2, sis)
+        eng.run(kernel=kern)
+        h, c = eng.histograms()
+        check_hist(h, c, ho, co, kern, 'edge catalogue')
+        assert c.sum() > 0
+
+
+@pytest.mark.parametrize('kern', KERNELS)
+def test_adversarial_bin_edges_bit_exact(kern):
+    """Pairs within a few ulps of an rt edge: the FP32 kernel must fall back to
+    the FP64 formula and land where the oracle does."""
+    fs, f1, f2, vb = E.cos_variant_cases(192)
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.set_pairs(f1, f2)
+        st = eng.run(kernel=kern)
+        h, c = eng.histograms()
+    got = np.array([int(np.nonzero(c[s])[0][0]) if c[s].sum() else -1 for s in range(len(f1))])
+    assert np.array_equal(got, vb[:, 0])
+    if kern == N.KERNEL_FP32_GUARDED:
+        assert st['guard_rechecks'] >= len(f1) // 2
+
+
+def test_guard_below_bound_is_rejected(cfg0):
+    fs, am, eng, _, _ = cfg0
+    with pytest.raises(N.LyaError) as e:
+        eng.run(kernel=N.KERNEL_FP32_GUARDED, guard=1e-7)
+    assert e.value.code == 6
+    eng.run(kernel=N.KERNEL_FP32_GUARDED, guard=1e-4)   # context still usable
+
+
+def test_errors_do_not_poison_context(cfg0):
+    fs, am, eng, _, _ = cfg0
+    with pytest.raises(N.LyaError):
+        eng.run(kernel=7)
+    with pytest.raises(N.LyaError):
+        eng.run(slots=(5, 2))
+    with pytest.raises(N.LyaError):
+        eng.set_pairs(np.array([0, fs.n + 5]), np.array([1, 2]))
+    eng.build_pairs(am)
+    eng.run()
+
+
+def test_unsorted_and_empty_forests_full_walk():
+    """Forests with decreasing dc are walked over every diagonal (no band
+    pruning) and still match the oracle."""
+    rng = np.random.default_rng(2)
+    fs = synthetic.make(4, n=60)
+    # reverse a third of the forests
+    for f in range(0, fs.n, 3):
+        a, b = fs.start[f], fs.start[f + 1]
+        for arr in (fs.dc, fs.w, fs.dw, fs.z, fs.dl):
+            arr[a:b] = arr[a:b][::-1].copy()
+    am = synthetic.angmax_for(fs)
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.build_pairs(am)
+        off, nbr = O.neighbours(fs, am)
+        f1, f2, sis, _ = O.items_from_csr(fs, off, nbr)
+        ho, co = O.corr(fs, f1, f2, sis)
+        for kern in KERNELS:
+            eng.run(kernel=kern)
+            h, c = eng.histograms()
+            check_hist(h, c, ho, co, kern, f'unsorted {kern}')
