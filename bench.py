@@ -306,15 +306,17 @@ def run_b200(args, dist):
         eng.run(kernel=kern, guard=GUARD)
         N.check(L.lya_corr_get(eng.ctx, 0, nslot, p(hist_out), p(cnt_out)), eng.ctx)
 
-    e2e_step()
-    dist.barrier()
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    for _ in range(args.e2e_steps):
+    e2e_value = None
+    if args.e2e_steps > 0:
         e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = dist.max(time.perf_counter() - t)
-    e2e_value = dist.sum(ref_pairs * args.e2e_steps) / e2e_s
+        dist.barrier()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = dist.max(time.perf_counter() - t)
+        e2e_value = dist.sum(ref_pairs * args.e2e_steps) / e2e_s
 
     out = None
     if dist.rank == 0:

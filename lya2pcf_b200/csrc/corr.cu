@@ -391,8 +391,9 @@ __device__ void item_diag(const CorrParams& p, int64_t t, const SmemHist& h, typ
             // rp crossing into the adjacent bin, rt unchanged: shift the run by one in rp
             if (!eyl && !eyh && r.bx >= 0) {
               const int nbx = exh ? r.bx + 1 : r.bx - 1;
-              const Real d = exh ? (Real)1 : (Real)-1;
-              const Real nlo = r.xlo + d, nhi = r.xhi + d;
+              // acceptance interval of bin nbx (the lower edge of bin 0 cannot be crossed)
+              const Real nlo = nbx == 0 ? -INF : (Real)nbx + gx;
+              const Real nhi = (Real)(nbx + 1) - gx;
               if (nbx >= 0 && nbx < np && x >= nlo && x < nhi) {
                 r.bx = nbx; r.xlo = nlo; r.xhi = nhi;
                 full = false;
