@@ -47,6 +47,7 @@ typedef struct {
   int32_t blocks_per_sm;   /* 0 = default (1) */
   int32_t slot_begin;      /* restrict the run to pairs whose first forest's */
   int32_t slot_end;        /* slot is in [slot_begin, slot_end); 0,0 = all    */
+  int32_t variant;         /* diagonal walk: 0 = two diagonals per lane, 1 = one */
 } lya_corr_opts;
 
 typedef struct {

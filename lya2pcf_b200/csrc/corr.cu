@@ -67,6 +67,7 @@ struct CorrParams {
   float gx, gy;        // guard half-widths in bin units (FP32 kernel)
   int cos_variant;
   int run_cap;
+  int variant;          // walk: 0 two diagonals per lane, 1 one diagonal per lane
   double* hist;                 // [slot][LYA_NQ][2][nb]
   unsigned long long* counts;   // [slot][nb]
   unsigned long long* stats;    // [ST_N]
@@ -141,7 +142,7 @@ __device__ void diagonal_band(int L1, int L2, const float4* __restrict__ P1, HiL
 // shared memory (plain stores, positions from a ballot); the warp drains the
 // buffer into the CTA histogram with all 32 lanes when it holds 32 records or
 // more, so the long-latency FP64 shared atomics never run in a divergent branch.
-constexpr int REC = 64;
+constexpr int REC = 128;   // records per warp buffer (up to 64 written per step)
 
 struct __align__(16) RecF32 {
   int bin, n;
@@ -439,6 +440,161 @@ __device__ void item_diag(const CorrParams& p, int64_t t, const SmemHist& h, typ
   }
 }
 
+// Two diagonals per lane: lane l walks diagonals m = mg + 2l and m + 1 at the
+// same f1 pixel i = base + k - l, so one pass covers 64 diagonals, the f1 pixel
+// serves both pairs and the second pair's f2 pixel at step k is the first
+// pair's at step k+1 (one f2 load per step).  Two independent runs per lane
+// give the scheduler two dependency chains.
+template <class Tr, bool GUARDED>
+__device__ void item_diag2(const CorrParams& p, int64_t t, const SmemHist& h, typename Tr::Rec* buf, int& cnt,
+                           LaneStats& st) {
+  using Real = typename Tr::Real;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int fa = p.f1[t], fb = p.f2[t];
+  const int L1 = p.len[fa], L2 = p.len[fb];
+  if (L1 <= 0 || L2 <= 0) return;
+  const int64_t a = p.pstart[fa], b = p.pstart[fb];
+  const int np = p.np, nt = p.nt, nb = p.nb;
+  double ch, sh;
+  pair_half_angles(p, fa, fb, ch, sh);
+  typename Tr::Geo geo;
+  if constexpr (GUARDED) {
+    geo.chb = __double2float_rn(ch * p.binner_rp);
+    geo.shb = __double2float_rn(sh * p.binner_rt);
+  } else {
+    geo.ch = ch; geo.sh = sh; geo.brp = p.binner_rp; geo.brt = p.binner_rt;
+  }
+  const Real gx = GUARDED ? (Real)p.gx : (Real)0, gy = GUARDED ? (Real)p.gy : (Real)0;
+  const bool srt = p.sorted[fa] && p.sorted[fb];
+  int m_lo = -(L1 - 1), m_hi = L2 - 1;
+  if (srt) {
+    const float4* __restrict__ P1 = p.pix4 + a;
+    const float4* __restrict__ P2 = p.pix4 + b;
+    const double slack = GUARDED ? 2.0 * p.gx : 1e-3;
+    const double rp_reach = ch > 0.0 ? ((double)np + slack) / (ch * p.binner_rp) : 1e300;
+    const double rt_reach = sh > 0.0 ? ((double)nt + slack) / (sh * p.binner_rt) : 1e300;
+    diagonal_band(L1, L2, P1, [&](int j) { return P2[j].x; }, rp_reach, rt_reach, m_lo, m_hi);
+  }
+  const Real INF = inf_of<Real>();
+  const Real ycut = (Real)nt + gy;
+  const int cap = p.run_cap;   // power of two
+  for (int mg = m_lo; mg <= m_hi; mg += 64) {
+    const int ma = mg + 2 * lane, mb = ma + 1;
+    // pair a: (i, i + ma), pair b: (i, i + mb); i = base + k - lane
+    const int ia_lo = max(0, -ma), ia_hi = (ma <= m_hi) ? min(L1, L2 - ma) : ia_lo;
+    const int ib_lo = max(0, -mb), ib_hi = (mb <= m_hi) ? min(L1, L2 - mb) : ib_lo;
+    const bool ne_a = ia_lo < ia_hi, ne_b = ib_lo < ib_hi;
+    int base = min(ne_a ? ia_lo + lane : INT_MAX, ne_b ? ib_lo + lane : INT_MAX);
+    for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
+    if (base == INT_MAX) continue;
+    const int ka_beg = ne_a ? ia_lo + lane - base : 0;
+    const int kb_beg = ne_b ? ib_lo + lane - base : 0;
+    int stop_a = ne_a ? ia_hi + lane - base : 0;
+    int stop_b = ne_b ? ib_hi + lane - base : 0;
+    int k_end = max(stop_a, stop_b);
+    for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
+    const int ioff = base - lane;             // i = ioff + k    (>= -31)
+    const int joff = base + ma - lane;        // j_a = joff + k  (>= -31), j_b = j_a + 1
+    const typename Tr::Ptr A1 = Tr::ptr(p, a + ioff);
+    const typename Tr::Ptr A2 = Tr::ptr(p, b + joff);
+    Run<Real> ra, rb;
+    ra.bx = -1; ra.by = -1; ra.k0 = 0; ra.xlo = INF; ra.xhi = -INF; ra.ylo = INF; ra.yhi = -INF;
+    rb = ra;
+    typename Tr::Acc acca, accb;
+    acca.zero();
+    accb.zero();
+    typename Tr::Pix q1 = Tr::load(A1, 0), q2a = Tr::load(A2, 0), q2b = Tr::load(A2, 1);
+    for (int k = 0; k < k_end; ++k) {
+      const typename Tr::Pix n1 = Tr::load(A1, k + 1), n2b = Tr::load(A2, k + 2);
+      bool act_a = k >= ka_beg && k < stop_a;
+      bool act_b = k >= kb_beg && k < stop_b;
+      Real xa, ya, rpa, rta, xb, yb, rpb, rtb;
+      Tr::coords(geo, q1, q2a, xa, ya, rpa, rta);
+      Tr::coords(geo, q1, q2b, xb, yb, rpb, rtb);
+      const bool exla = xa < ra.xlo, exha = !(xa < ra.xhi), eyla = ya < ra.ylo, eyha = !(ya < ra.yhi);
+      const bool exlb = xb < rb.xlo, exhb = !(xb < rb.xhi), eylb = yb < rb.ylo, eyhb = !(yb < rb.yhi);
+      const bool slow_a = act_a && (exla || exha || eyla || eyha);
+      const bool slow_b = act_b && (exlb || exhb || eylb || eyhb);
+      if (__any_sync(FULL, slow_a || slow_b)) {
+        close_runs<Tr>(slow_a, ra, acca, k, nt, buf, cnt, lt, st);
+        close_runs<Tr>(slow_b, rb, accb, k, nt, buf, cnt, lt, st);
+        if (slow_a) {
+          acca.zero();
+          ra.k0 = k;
+          bool full = true;
+          if (!eyla && !eyha && ra.bx >= 0) {
+            const int nbx = exha ? ra.bx + 1 : ra.bx - 1;
+            const Real nlo = nbx == 0 ? -INF : (Real)nbx + gx;
+            const Real nhi = (Real)(nbx + 1) - gx;
+            if (nbx >= 0 && nbx < np && xa >= nlo && xa < nhi) {
+              ra.bx = nbx; ra.xlo = nlo; ra.xhi = nhi;
+              full = false;
+            }
+          }
+          if (full) {
+            if (srt && ya >= ycut) {
+              stop_a = k; act_a = false; ra.bx = -1;
+            } else {
+              classify<Real>(p, ra, xa, ya, gx, gy, p.pix8 + a + ioff + k, p.pix8 + b + joff + k, ch, sh, st);
+            }
+          }
+        }
+        if (slow_b) {
+          accb.zero();
+          rb.k0 = k;
+          bool full = true;
+          if (!eylb && !eyhb && rb.bx >= 0) {
+            const int nbx = exhb ? rb.bx + 1 : rb.bx - 1;
+            const Real nlo = nbx == 0 ? -INF : (Real)nbx + gx;
+            const Real nhi = (Real)(nbx + 1) - gx;
+            if (nbx >= 0 && nbx < np && xb >= nlo && xb < nhi) {
+              rb.bx = nbx; rb.xlo = nlo; rb.xhi = nhi;
+              full = false;
+            }
+          }
+          if (full) {
+            if (srt && yb >= ycut) {
+              stop_b = k; act_b = false; rb.bx = -1;
+            } else {
+              classify<Real>(p, rb, xb, yb, gx, gy, p.pix8 + a + ioff + k, p.pix8 + b + joff + k + 1, ch, sh, st);
+            }
+          }
+        }
+        if (cnt > REC - 64) {
+          drain(buf, cnt, h, nb, st);
+          cnt = 0;
+        }
+      }
+      if (act_a) acca.add(q1, q2a, xa, ya, rpa, rta);
+      if (act_b) accb.add(q1, q2b, xb, yb, rpb, rtb);
+      q1 = n1;
+      q2a = q2b;
+      q2b = n2b;
+      if ((k & (cap - 1)) == cap - 1) {   // bound the length of a register sum
+        const bool live_a = k >= ka_beg && k < stop_a, live_b = k >= kb_beg && k < stop_b;
+        close_runs<Tr>(live_a, ra, acca, k + 1, nt, buf, cnt, lt, st);
+        close_runs<Tr>(live_b, rb, accb, k + 1, nt, buf, cnt, lt, st);
+        if (live_a) { acca.zero(); ra.k0 = k + 1; }
+        if (live_b) { accb.zero(); rb.k0 = k + 1; }
+        if (cnt > REC - 64) {
+          drain(buf, cnt, h, nb, st);
+          cnt = 0;
+        }
+        if (__all_sync(FULL, k + 1 >= stop_a && k + 1 >= stop_b)) break;
+      }
+    }
+    const int kfa = min(stop_a, k_end), kfb = min(stop_b, k_end);
+    st.evaluated += (unsigned long long)(max(0, kfa - ka_beg) + max(0, kfb - kb_beg));
+    close_runs<Tr>(true, ra, acca, max(kfa, ra.k0), nt, buf, cnt, lt, st);
+    close_runs<Tr>(true, rb, accb, max(kfb, rb.k0), nt, buf, cnt, lt, st);
+    if (cnt > REC - 64) {
+      drain(buf, cnt, h, nb, st);
+      cnt = 0;
+    }
+  }
+}
+
 // ------------------------------------------------------------------ FP64 plain (every pixel pair)
 __device__ void item_plain(const CorrParams& p, int64_t t, const SmemHist& h, LaneStats& st) {
   const int lane = threadIdx.x & 31;
@@ -527,10 +683,13 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
       if (lane == 0) t = atomicAdd(&s_next, 1ull);
       t = __shfl_sync(FULL, t, 0);
       if ((int64_t)t >= seg_end) break;
-      if (KIND == LYA_KERNEL_FP32_GUARDED)
-        item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
-      else if (KIND == LYA_KERNEL_FP64_DIAGONAL)
-        item_diag<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
+      if (KIND == LYA_KERNEL_FP32_GUARDED) {
+        if (p.variant == 1) item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+        else item_diag2<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+      } else if (KIND == LYA_KERNEL_FP64_DIAGONAL) {
+        if (p.variant == 1) item_diag<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
+        else item_diag2<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
+      }
       else item_plain(p, (int64_t)t, h, st);
     }
     if (KIND == LYA_KERNEL_FP32_GUARDED) drain(reinterpret_cast<RecF32*>(mybuf), cnt, h, nb, st);
@@ -719,6 +878,7 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
   p.gx = (float)gx_bins; p.gy = (float)gy_bins;
   p.cos_variant = ctx->cos_variant;
   p.run_cap = 128;
+  p.variant = o->variant;
   p.hist = ctx->hist; p.counts = ctx->counts; p.stats = ctx->stats;
 
   cudaError_t e = cudaSuccess;
@@ -761,6 +921,7 @@ extern "C" int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts) {
   if (opts) o = *opts;
   if (o.kernel < 0 || o.kernel > 2) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: unknown kernel %d", o.kernel);
   if (o.blocks_per_sm < 0 || o.blocks_per_sm > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: blocks_per_sm must be 0 or 1");
+  if (o.variant < 0 || o.variant > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant must be 0 or 1");
   if (o.warps_per_block != 0 && o.warps_per_block != 16)
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: warps_per_block must be 0 or 16");
   if (o.slot_begin < 0 || o.slot_end < o.slot_begin || o.slot_end > ctx->cat.n_slots)

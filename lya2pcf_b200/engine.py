@@ -109,11 +109,11 @@ class PairEngine:
         return f1[:self.n_pairs], f2[:self.n_pairs]
 
     # ------------------------------------------------------------------ correlation
-    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0, slots=None):
+    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0, slots=None, variant=0):
         """Histograms of the work queue (restricted to owner slots
         ``range(*slots)`` when given).  Returns :meth:`stats`."""
         s0, s1 = (0, 0) if slots is None else (int(slots[0]), int(slots[1]))
-        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), s0, s1)
+        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), s0, s1, int(variant))
         self._check(self.lib.lya_corr_run(self.ctx, C.byref(opts)))
         return self.stats()
 
