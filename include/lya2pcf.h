@@ -134,6 +134,28 @@ int lya_update_weights(lya_ctx* ctx, const double* w, const double* dw, int32_t 
 
 int lya_stats(lya_ctx* ctx, lya_stats_t* out);
 
+/* Histograms of one owner pixel without any device allocation.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory (device memory owned by another framework's caching allocator, a
+ * fixed device-memory budget, allocation calls that must stay out of a
+ * recorded sequence).  Every pointer is caller-owned device memory on
+ * `device`: the catalogue as unpadded CSR (forest f owns pixels
+ * start[f]..start[f+1]-1 of dc, w, dw, z), unit vectors ux, uy, uz per forest,
+ * and the forest pairs (f1[k], f2[k]), all binned into one histogram;
+ * outputs hist[LYA_NQ][np*nt] (FP64, same quantities as lya_corr_get) and
+ * counts[np*nt], both overwritten.  Every pixel pair is evaluated with the
+ * reference FP64 formula (the FP64 plain kernel).  The only scratch is a
+ * file-scope device array of 4096 bins (320 KB per GPU that loads the
+ * library, kept until exit): np*nt above 4096 is rejected with LYA_ERR_ARG.
+ * The first call on a device resolves the array's device address and should
+ * come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race.  stream: a cudaStream_t, or NULL for the default
+ * stream.  The call is asynchronous on that stream. */
+int lya_corr_pixel_noalloc(int device, const double* dc, const double* w, const double* dw, const double* z,
+                           const int64_t* start, const double* ux, const double* uy, const double* uz,
+                           const int32_t* f1, const int32_t* f2, int64_t n_pairs, double rpmax, double rtmax,
+                           int32_t np, int32_t nt, double* hist, uint64_t* counts, void* stream);
+
 /* Device timer on the context's stream: op 0 records the start event, op 1
  * records the stop event, waits for it and writes the elapsed milliseconds. */
 int lya_timer(lya_ctx* ctx, int32_t op, double* ms);
