@@ -47,7 +47,8 @@ typedef struct {
   int32_t blocks_per_sm;   /* 0 = default (1) */
   int32_t slot_begin;      /* restrict the run to pairs whose first forest's */
   int32_t slot_end;        /* slot is in [slot_begin, slot_end); 0,0 = all    */
-  int32_t variant;         /* diagonal walk: 0 = two diagonals per lane, 1 = one */
+  int32_t variant;         /* diagonal walk: 0 = default (FP32: two diagonals per
+                              lane, FP64: one), 1 = one per lane, 2 = two */
 } lya_corr_opts;
 
 typedef struct {

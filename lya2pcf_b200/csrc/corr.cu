@@ -67,7 +67,7 @@ struct CorrParams {
   float gx, gy;        // guard half-widths in bin units (FP32 kernel)
   int cos_variant;
   int run_cap;
-  int variant;          // walk: 0 two diagonals per lane, 1 one diagonal per lane
+  int variant;          // walk: 0 default, 1 one diagonal per lane, 2 two diagonals per lane
   double* hist;                 // [slot][LYA_NQ][2][nb]
   unsigned long long* counts;   // [slot][nb]
   unsigned long long* stats;    // [ST_N]
@@ -444,41 +444,153 @@ __device__ void item_diag(const CorrParams& p, int64_t t, const SmemHist& h, typ
 // same f1 pixel i = base + k - l, so one pass covers 64 diagonals, the f1 pixel
 // serves both pairs and the second pair's f2 pixel at step k is the first
 // pair's at step k+1 (one f2 load per step).  Two independent runs per lane
-// give the scheduler two dependency chains.
+// give the scheduler two dependency chains.  A bin change costs a predicated
+// record store and, for an rp crossing into the adjacent bin, a predicated
+// shift of the run; only rt crossings (warp-synchronous), guard-band pairs and
+// range changes take the warp-voted full classification.
+template <class Tr>
+struct Walk2 {
+  using Real = typename Tr::Real;
+  using Pix = typename Tr::Pix;
+  const CorrParams& p;
+  const SmemHist& h;
+  typename Tr::Rec* buf;
+  int& cnt;
+  LaneStats& st;
+  typename Tr::Geo geo;
+  Real gx, gy, ycut, INF;
+  int np, nt, nb;
+  unsigned lt;
+  bool srt;
+  const double4* __restrict__ D1;   // FP64 pixels of f1 at i = 0 (guard recheck)
+  const double4* __restrict__ D2;   // FP64 pixels of f2 at j = 0
+  double ch, sh;
+  int ioff, joff;
+  int ka_beg, kb_beg, stop_a, stop_b;
+  Run<Real> ra, rb;
+  typename Tr::Acc acca, accb;
+
+  __device__ __forceinline__ void record(bool w, const Run<Real>& r, const typename Tr::Acc& acc, int k,
+                                         unsigned bal, int base_pos) {
+    if (w) {
+      typename Tr::Rec rec;
+      rec.bin = r.bx * nt + r.by; rec.n = k - r.k0;
+      rec.aw = acc.aw; rec.adw = acc.adw; rec.ax = acc.ax; rec.ay = acc.ay; rec.az = acc.az;
+      buf[base_pos + __popc(bal & lt)] = rec;
+    }
+  }
+
+  // rp crossing into the adjacent bin with rt unchanged: returns true when the
+  // run could be shifted (the pair lies inside the new bin's acceptance interval)
+  __device__ __forceinline__ bool shift(Run<Real>& r, bool slow, bool eyl, bool eyh, bool exh, Real x) {
+    const int nbx = exh ? r.bx + 1 : r.bx - 1;
+    const Real nlo = nbx == 0 ? -INF : (Real)nbx + gx;
+    const Real nhi = (Real)(nbx + 1) - gx;
+    const bool ok = slow && !eyl && !eyh && r.bx >= 0 && (unsigned)nbx < (unsigned)np && x >= nlo && x < nhi;
+    r.bx = ok ? nbx : r.bx;
+    r.xlo = ok ? nlo : r.xlo;
+    r.xhi = ok ? nhi : r.xhi;
+    return ok;
+  }
+
+  __device__ __forceinline__ void full(Run<Real>& r, int& stop, bool& act, int k, Real x, Real y, int joff_pair) {
+    if (srt && y >= ycut) {   // rt only grows along a sorted diagonal: the lane's diagonal is done
+      stop = k;
+      act = false;
+      r.bx = -1;
+    } else {
+      classify<Real>(p, r, x, y, gx, gy, D1 + ioff + k, D2 + joff_pair + k, ch, sh, st);
+    }
+  }
+
+  __device__ __forceinline__ void step(int k, const Pix& q1, const Pix& q2a, const Pix& q2b) {
+    bool act_a = k >= ka_beg && k < stop_a;
+    bool act_b = k >= kb_beg && k < stop_b;
+    Real xa, ya, rpa, rta, xb, yb, rpb, rtb;
+    Tr::coords(geo, q1, q2a, xa, ya, rpa, rta);
+    Tr::coords(geo, q1, q2b, xb, yb, rpb, rtb);
+    const bool exha = !(xa < ra.xhi), eyla = ya < ra.ylo, eyha = !(ya < ra.yhi);
+    const bool exhb = !(xb < rb.xhi), eylb = yb < rb.ylo, eyhb = !(yb < rb.yhi);
+    const bool slow_a = act_a && (xa < ra.xlo || exha || eyla || eyha);
+    const bool slow_b = act_b && (xb < rb.xlo || exhb || eylb || eyhb);
+    if (__any_sync(FULL, slow_a || slow_b)) {
+      const bool wa = slow_a && ra.bx >= 0 && k > ra.k0;
+      const bool wb = slow_b && rb.bx >= 0 && k > rb.k0;
+      const unsigned bala = __ballot_sync(FULL, wa), balb = __ballot_sync(FULL, wb);
+      record(wa, ra, acca, k, bala, cnt);
+      record(wb, rb, accb, k, balb, cnt + __popc(bala));
+      cnt += __popc(bala) + __popc(balb);
+      const bool fa = slow_a && !shift(ra, slow_a, eyla, eyha, exha, xa);
+      const bool fb = slow_b && !shift(rb, slow_b, eylb, eyhb, exhb, xb);
+      if (slow_a) { acca.zero(); ra.k0 = k; }
+      if (slow_b) { accb.zero(); rb.k0 = k; }
+      if (__any_sync(FULL, fa || fb)) {
+        if (fa) full(ra, stop_a, act_a, k, xa, ya, joff);
+        if (fb) full(rb, stop_b, act_b, k, xb, yb, joff + 1);
+      }
+      if (cnt > REC - 64) {
+        drain(buf, cnt, h, nb, st);
+        cnt = 0;
+      }
+    }
+    if (act_a) acca.add(q1, q2a, xa, ya, rpa, rta);
+    if (act_b) accb.add(q1, q2b, xb, yb, rpb, rtb);
+  }
+
+  // close both runs at step k (all lanes in `live_*`), records for in-range ones
+  __device__ __forceinline__ void close(bool live_a, bool live_b, int ka, int kb) {
+    const bool wa = live_a && ra.bx >= 0 && ka > ra.k0;
+    const bool wb = live_b && rb.bx >= 0 && kb > rb.k0;
+    const unsigned bala = __ballot_sync(FULL, wa), balb = __ballot_sync(FULL, wb);
+    record(wa, ra, acca, ka, bala, cnt);
+    record(wb, rb, accb, kb, balb, cnt + __popc(bala));
+    cnt += __popc(bala) + __popc(balb);
+    if (live_a) { acca.zero(); ra.k0 = ka; }
+    if (live_b) { accb.zero(); rb.k0 = kb; }
+    if (cnt > REC - 64) {
+      drain(buf, cnt, h, nb, st);
+      cnt = 0;
+    }
+  }
+};
+
 template <class Tr, bool GUARDED>
 __device__ void item_diag2(const CorrParams& p, int64_t t, const SmemHist& h, typename Tr::Rec* buf, int& cnt,
                            LaneStats& st) {
   using Real = typename Tr::Real;
+  using Pix = typename Tr::Pix;
   const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
   const int fa = p.f1[t], fb = p.f2[t];
   const int L1 = p.len[fa], L2 = p.len[fb];
   if (L1 <= 0 || L2 <= 0) return;
   const int64_t a = p.pstart[fa], b = p.pstart[fb];
-  const int np = p.np, nt = p.nt, nb = p.nb;
-  double ch, sh;
-  pair_half_angles(p, fa, fb, ch, sh);
-  typename Tr::Geo geo;
+  Walk2<Tr> W{p, h, buf, cnt, st};
+  W.np = p.np; W.nt = p.nt; W.nb = p.nb;
+  W.lt = (1u << lane) - 1u;
+  pair_half_angles(p, fa, fb, W.ch, W.sh);
   if constexpr (GUARDED) {
-    geo.chb = __double2float_rn(ch * p.binner_rp);
-    geo.shb = __double2float_rn(sh * p.binner_rt);
+    W.geo.chb = __double2float_rn(W.ch * p.binner_rp);
+    W.geo.shb = __double2float_rn(W.sh * p.binner_rt);
   } else {
-    geo.ch = ch; geo.sh = sh; geo.brp = p.binner_rp; geo.brt = p.binner_rt;
+    W.geo.ch = W.ch; W.geo.sh = W.sh; W.geo.brp = p.binner_rp; W.geo.brt = p.binner_rt;
   }
-  const Real gx = GUARDED ? (Real)p.gx : (Real)0, gy = GUARDED ? (Real)p.gy : (Real)0;
-  const bool srt = p.sorted[fa] && p.sorted[fb];
+  W.gx = GUARDED ? (Real)p.gx : (Real)0;
+  W.gy = GUARDED ? (Real)p.gy : (Real)0;
+  W.INF = inf_of<Real>();
+  W.ycut = (Real)W.nt + W.gy;
+  W.srt = p.sorted[fa] && p.sorted[fb];
+  W.D1 = p.pix8 + a;
+  W.D2 = p.pix8 + b;
   int m_lo = -(L1 - 1), m_hi = L2 - 1;
-  if (srt) {
+  if (W.srt) {
     const float4* __restrict__ P1 = p.pix4 + a;
     const float4* __restrict__ P2 = p.pix4 + b;
     const double slack = GUARDED ? 2.0 * p.gx : 1e-3;
-    const double rp_reach = ch > 0.0 ? ((double)np + slack) / (ch * p.binner_rp) : 1e300;
-    const double rt_reach = sh > 0.0 ? ((double)nt + slack) / (sh * p.binner_rt) : 1e300;
+    const double rp_reach = W.ch > 0.0 ? ((double)W.np + slack) / (W.ch * p.binner_rp) : 1e300;
+    const double rt_reach = W.sh > 0.0 ? ((double)W.nt + slack) / (W.sh * p.binner_rt) : 1e300;
     diagonal_band(L1, L2, P1, [&](int j) { return P2[j].x; }, rp_reach, rt_reach, m_lo, m_hi);
   }
-  const Real INF = inf_of<Real>();
-  const Real ycut = (Real)nt + gy;
-  const int cap = p.run_cap;   // power of two
+  const int cap = p.run_cap;   // power of two, even
   for (int mg = m_lo; mg <= m_hi; mg += 64) {
     const int ma = mg + 2 * lane, mb = ma + 1;
     // pair a: (i, i + ma), pair b: (i, i + mb); i = base + k - lane
@@ -488,110 +600,42 @@ __device__ void item_diag2(const CorrParams& p, int64_t t, const SmemHist& h, ty
     int base = min(ne_a ? ia_lo + lane : INT_MAX, ne_b ? ib_lo + lane : INT_MAX);
     for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
     if (base == INT_MAX) continue;
-    const int ka_beg = ne_a ? ia_lo + lane - base : 0;
-    const int kb_beg = ne_b ? ib_lo + lane - base : 0;
-    int stop_a = ne_a ? ia_hi + lane - base : 0;
-    int stop_b = ne_b ? ib_hi + lane - base : 0;
-    int k_end = max(stop_a, stop_b);
+    W.ka_beg = ne_a ? ia_lo + lane - base : 0;
+    W.kb_beg = ne_b ? ib_lo + lane - base : 0;
+    W.stop_a = ne_a ? ia_hi + lane - base : 0;
+    W.stop_b = ne_b ? ib_hi + lane - base : 0;
+    int k_end = max(W.stop_a, W.stop_b);
     for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
-    const int ioff = base - lane;             // i = ioff + k    (>= -31)
-    const int joff = base + ma - lane;        // j_a = joff + k  (>= -31), j_b = j_a + 1
-    const typename Tr::Ptr A1 = Tr::ptr(p, a + ioff);
-    const typename Tr::Ptr A2 = Tr::ptr(p, b + joff);
-    Run<Real> ra, rb;
-    ra.bx = -1; ra.by = -1; ra.k0 = 0; ra.xlo = INF; ra.xhi = -INF; ra.ylo = INF; ra.yhi = -INF;
-    rb = ra;
-    typename Tr::Acc acca, accb;
-    acca.zero();
-    accb.zero();
-    typename Tr::Pix q1 = Tr::load(A1, 0), q2a = Tr::load(A2, 0), q2b = Tr::load(A2, 1);
-    for (int k = 0; k < k_end; ++k) {
-      const typename Tr::Pix n1 = Tr::load(A1, k + 1), n2b = Tr::load(A2, k + 2);
-      bool act_a = k >= ka_beg && k < stop_a;
-      bool act_b = k >= kb_beg && k < stop_b;
-      Real xa, ya, rpa, rta, xb, yb, rpb, rtb;
-      Tr::coords(geo, q1, q2a, xa, ya, rpa, rta);
-      Tr::coords(geo, q1, q2b, xb, yb, rpb, rtb);
-      const bool exla = xa < ra.xlo, exha = !(xa < ra.xhi), eyla = ya < ra.ylo, eyha = !(ya < ra.yhi);
-      const bool exlb = xb < rb.xlo, exhb = !(xb < rb.xhi), eylb = yb < rb.ylo, eyhb = !(yb < rb.yhi);
-      const bool slow_a = act_a && (exla || exha || eyla || eyha);
-      const bool slow_b = act_b && (exlb || exhb || eylb || eyhb);
-      if (__any_sync(FULL, slow_a || slow_b)) {
-        close_runs<Tr>(slow_a, ra, acca, k, nt, buf, cnt, lt, st);
-        close_runs<Tr>(slow_b, rb, accb, k, nt, buf, cnt, lt, st);
-        if (slow_a) {
-          acca.zero();
-          ra.k0 = k;
-          bool full = true;
-          if (!eyla && !eyha && ra.bx >= 0) {
-            const int nbx = exha ? ra.bx + 1 : ra.bx - 1;
-            const Real nlo = nbx == 0 ? -INF : (Real)nbx + gx;
-            const Real nhi = (Real)(nbx + 1) - gx;
-            if (nbx >= 0 && nbx < np && xa >= nlo && xa < nhi) {
-              ra.bx = nbx; ra.xlo = nlo; ra.xhi = nhi;
-              full = false;
-            }
-          }
-          if (full) {
-            if (srt && ya >= ycut) {
-              stop_a = k; act_a = false; ra.bx = -1;
-            } else {
-              classify<Real>(p, ra, xa, ya, gx, gy, p.pix8 + a + ioff + k, p.pix8 + b + joff + k, ch, sh, st);
-            }
-          }
-        }
-        if (slow_b) {
-          accb.zero();
-          rb.k0 = k;
-          bool full = true;
-          if (!eylb && !eyhb && rb.bx >= 0) {
-            const int nbx = exhb ? rb.bx + 1 : rb.bx - 1;
-            const Real nlo = nbx == 0 ? -INF : (Real)nbx + gx;
-            const Real nhi = (Real)(nbx + 1) - gx;
-            if (nbx >= 0 && nbx < np && xb >= nlo && xb < nhi) {
-              rb.bx = nbx; rb.xlo = nlo; rb.xhi = nhi;
-              full = false;
-            }
-          }
-          if (full) {
-            if (srt && yb >= ycut) {
-              stop_b = k; act_b = false; rb.bx = -1;
-            } else {
-              classify<Real>(p, rb, xb, yb, gx, gy, p.pix8 + a + ioff + k, p.pix8 + b + joff + k + 1, ch, sh, st);
-            }
-          }
-        }
-        if (cnt > REC - 64) {
-          drain(buf, cnt, h, nb, st);
-          cnt = 0;
-        }
-      }
-      if (act_a) acca.add(q1, q2a, xa, ya, rpa, rta);
-      if (act_b) accb.add(q1, q2b, xb, yb, rpb, rtb);
-      q1 = n1;
-      q2a = q2b;
-      q2b = n2b;
-      if ((k & (cap - 1)) == cap - 1) {   // bound the length of a register sum
-        const bool live_a = k >= ka_beg && k < stop_a, live_b = k >= kb_beg && k < stop_b;
-        close_runs<Tr>(live_a, ra, acca, k + 1, nt, buf, cnt, lt, st);
-        close_runs<Tr>(live_b, rb, accb, k + 1, nt, buf, cnt, lt, st);
-        if (live_a) { acca.zero(); ra.k0 = k + 1; }
-        if (live_b) { accb.zero(); rb.k0 = k + 1; }
-        if (cnt > REC - 64) {
-          drain(buf, cnt, h, nb, st);
-          cnt = 0;
-        }
-        if (__all_sync(FULL, k + 1 >= stop_a && k + 1 >= stop_b)) break;
+    W.ioff = base - lane;             // i = ioff + k    (>= -31)
+    W.joff = base + ma - lane;        // j_a = joff + k  (>= -31), j_b = j_a + 1
+    const typename Tr::Ptr A1 = Tr::ptr(p, a + W.ioff);
+    const typename Tr::Ptr A2 = Tr::ptr(p, b + W.joff);
+    W.ra.bx = -1; W.ra.by = -1; W.ra.k0 = 0;
+    W.ra.xlo = W.INF; W.ra.xhi = -W.INF; W.ra.ylo = W.INF; W.ra.yhi = -W.INF;
+    W.rb = W.ra;
+    W.acca.zero();
+    W.accb.zero();
+    // pixels of steps k (q1a, q2x, q2y); the loop body handles two steps so the
+    // registers rotate without copies
+    Pix q1a = Tr::load(A1, 0), q2x = Tr::load(A2, 0), q2y = Tr::load(A2, 1);
+    int k = 0;
+    for (; k < k_end; k += 2) {
+      const Pix q1b = Tr::load(A1, k + 1), q2z = Tr::load(A2, k + 2);
+      W.step(k, q1a, q2x, q2y);
+      q1a = Tr::load(A1, k + 2);
+      q2x = Tr::load(A2, k + 3);
+      if (k + 1 < k_end) W.step(k + 1, q1b, q2y, q2z);
+      // now q1a = f1[k+2], q2x = f2[k+3]; the next pair of steps wants (f2[k+2], f2[k+3])
+      q2y = q2x;
+      q2x = q2z;
+      if (((k + 2) & (cap - 1)) == 0) {   // bound the length of a register sum
+        W.close(k + 1 >= W.ka_beg && k + 1 < W.stop_a, k + 1 >= W.kb_beg && k + 1 < W.stop_b, k + 2, k + 2);
+        if (__all_sync(FULL, k + 2 >= W.stop_a && k + 2 >= W.stop_b)) { k += 2; break; }
       }
     }
-    const int kfa = min(stop_a, k_end), kfb = min(stop_b, k_end);
-    st.evaluated += (unsigned long long)(max(0, kfa - ka_beg) + max(0, kfb - kb_beg));
-    close_runs<Tr>(true, ra, acca, max(kfa, ra.k0), nt, buf, cnt, lt, st);
-    close_runs<Tr>(true, rb, accb, max(kfb, rb.k0), nt, buf, cnt, lt, st);
-    if (cnt > REC - 64) {
-      drain(buf, cnt, h, nb, st);
-      cnt = 0;
-    }
+    const int kfa = min(W.stop_a, k_end), kfb = min(W.stop_b, k_end);
+    st.evaluated += (unsigned long long)(max(0, kfa - W.ka_beg) + max(0, kfb - W.kb_beg));
+    W.close(true, true, max(kfa, W.ra.k0), max(kfb, W.rb.k0));
   }
 }
 
@@ -687,8 +731,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
         if (p.variant == 1) item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
         else item_diag2<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
       } else if (KIND == LYA_KERNEL_FP64_DIAGONAL) {
-        if (p.variant == 1) item_diag<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
-        else item_diag2<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
+        if (p.variant == 2) item_diag2<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
+        else item_diag<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
       }
       else item_plain(p, (int64_t)t, h, st);
     }
@@ -921,7 +965,7 @@ extern "C" int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts) {
   if (opts) o = *opts;
   if (o.kernel < 0 || o.kernel > 2) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: unknown kernel %d", o.kernel);
   if (o.blocks_per_sm < 0 || o.blocks_per_sm > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: blocks_per_sm must be 0 or 1");
-  if (o.variant < 0 || o.variant > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant must be 0 or 1");
+  if (o.variant < 0 || o.variant > 2) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant must be 0, 1 or 2");
   if (o.warps_per_block != 0 && o.warps_per_block != 16)
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: warps_per_block must be 0 or 16");
   if (o.slot_begin < 0 || o.slot_end < o.slot_begin || o.slot_end > ctx->cat.n_slots)
