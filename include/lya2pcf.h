@@ -133,6 +133,17 @@ int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* gra
  * (fill_dw of forest_class.py:48-68 changes dw when delta or w change). */
 int lya_update_weights(lya_ctx* ctx, const double* w, const double* dw, int32_t device_ptrs);
 
+/* Distortion-matrix numerator D[np*nt][np*nt] and bin weights W[np*nt]
+ * (FP64, host arrays, overwritten) summed over the work queue (build it with
+ * lya_build_pairs, or pass the reference's subsampled neighbour lists with
+ * lya_set_pairs); replaces distortion_per_pixel
+ * (distortion_procedures_pycuda.py:195-279) and the kernels
+ * precompute_distances, compute_etas, order_active, compute_d
+ * (cuda_kernels.cpp:46-87, 165-278).  The normalised matrix of distortion.py:125
+ * is D / W[:, None].  Needs dl, omega and odl2 at upload; a pixel whose
+ * partners fall in more than 6 rt bins is reported as LYA_ERR_DATA. */
+int lya_dist_run(lya_ctx* ctx, double* D, double* W);
+
 int lya_stats(lya_ctx* ctx, lya_stats_t* out);
 
 /* Histograms of one owner pixel without any device allocation.  No

@@ -1,0 +1,356 @@
+// Distortion-matrix numerator of the lya2pcf B200 library.
+//
+// Reference: distortion_per_pixel (distortion_procedures_pycuda.py:195-279)
+// with the kernels precompute_distances, compute_etas, order_active and
+// compute_d (cuda_kernels.cpp:46-87, 165-278).  For a forest pair (f1, f2)
+// and pixel pairs (i, j) in bin A, (k, l) in bin B, with
+//   eta1_ik = delta_ik - w_k/Om1 - dl_i w_k dl_k / O1,   O = sum w dl^2,
+// the reference scatters, per in-range pair and per active bin B,
+//   D_AB += w_i w_j sum_{(k,l) in B} eta1_ik eta2_jl.
+//
+// This kernel evaluates the same sum in factored form.  With per-pixel columns
+//   S2[A,i] = sum_{j:(i,j) in A} w_j,   L2[A,i] = sum_{j:(i,j) in A} w_j dl_j
+//   S1[A,j] = sum_{i:(i,j) in A} w_i,   L1[A,j] = sum_{i:(i,j) in A} w_i dl_i
+// and per-bin moments M0_A = sum w_i w_j, Mi_A = sum w_i dl_i w_j,
+// Mj_A = sum w_i w_j dl_j, Mij_A = sum w_i dl_i w_j dl_j (over (i,j) in A):
+//   D_AB = [A==B] M0_A
+//        + M0_A M0_B/(Om1 Om2) + Mj_A Mj_B/(Om1 O2) + Mi_A Mi_B/(O1 Om2) + Mij_A Mij_B/(O1 O2)
+//        - sum_i w_i (S2[A,i] S2[B,i]/Om2 + L2[A,i] L2[B,i]/O2)
+//        - sum_j w_j (S1[A,j] S1[B,j]/Om1 + L1[A,j] L1[B,j]/O1)
+// (expand eta1_ik eta2_jl; the delta terms give the diagonal, the products of
+// the two projections the rank-4 part, the cross terms the columns).  The
+// column of a pixel spans a few rt bins only, so the column products are
+// 50x50 dense blocks (rp x rp) per pair of rt bins.
+//
+// One CTA per forest pair (grid-stride).  Bins come from the reference FP64
+// formula.  Columns live in CTA-private global scratch (a thread owns a pixel,
+// no atomics), moments in shared memory; D (np*nt squared FP64, 50 MB for 50x50
+// bins, L2-resident) receives one atomic add per touched entry per forest pair.
+// A forest whose sum w dl^2 is 0 has no slope to project out: its slope terms
+// are 0.
+#include <algorithm>
+#include <cmath>
+
+#include "lya_internal.cuh"
+
+namespace {
+
+constexpr int DT = 256;       // threads per CTA
+constexpr int TS = 6;         // rt bins a pixel column may span
+constexpr int NW = DT / 32;   // warps per CTA
+
+struct DistParams {
+  const double4* __restrict__ pix8;   // (dc, w, dw, z)
+  const double* __restrict__ dl;
+  const int64_t* __restrict__ pstart;
+  const int32_t* __restrict__ len;
+  const uint8_t* __restrict__ sorted;
+  const double* __restrict__ ux;
+  const double* __restrict__ uy;
+  const double* __restrict__ uz;
+  const double* __restrict__ omega;
+  const double* __restrict__ odl2;
+  const int32_t* __restrict__ f1;
+  const int32_t* __restrict__ f2;
+  int64_t n_items;
+  int max_len;
+  double binner_rp, binner_rt;
+  int np, nt, nb, cos_variant;
+  double* col;             // scratch [grid][2 sides][max_len][TS][np] x {S, L}
+  double* D;               // [nb][nb]
+  double* W;               // [nb]
+  unsigned long long* err; // [1] pixels whose column spans more than TS rt bins
+};
+
+__device__ __forceinline__ int pair_bin(double d1, double d2, double ch, double sh, const DistParams& p) {
+  const double rp = __dmul_rn(fabs(__dsub_rn(d1, d2)), ch);
+  const double rt = __dmul_rn(__dadd_rn(d1, d2), sh);
+  const double fp = floor(__dmul_rn(rp, p.binner_rp));
+  const double ft = floor(__dmul_rn(rt, p.binner_rt));
+  if (fp >= 0.0 && fp < (double)p.np && ft >= 0.0 && ft < (double)p.nt) return (int)fp * p.nt + (int)ft;
+  return -1;
+}
+
+__global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int ML = p.max_len;
+  const int np = p.np, nt = p.nt, nb = p.nb;
+  double* sd = reinterpret_cast<double*>(smem);          // [2][ML] dc
+  double* sw = sd + 2 * ML;                              // [2][ML] w
+  double* sl = sw + 2 * ML;                              // [2][ML] dl
+  double* mom = sl + 2 * ML;                             // [4][nb] moments of the touched bins
+  double* wcol = mom + 4 * nb;                           // [NW][2][TS*np] a warp's column being built
+  int* tlo = reinterpret_cast<int*>(wcol + NW * 2 * TS * np);   // [2][ML]
+  int* span = tlo + 2 * ML;                              // [2][ML]
+  int* tcount = span + 2 * ML;                           // [nt + 1]
+  int* tfill = tcount + (nt + 1);                        // [nt + 1]
+  int* tlist = tfill + (nt + 1);                         // [2*ML*TS] packed (side << 16 | pixel)
+  int* nzlist = tlist + 2 * ML * TS;                     // [nb]
+  __shared__ int s_T0, s_T1, s_nnz, s_maxspan;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* colS = p.col + (size_t)blockIdx.x * 2 * 2 * ML * TS * np;   // [2 sides][ML][TS][np]
+  double* colL = colS + (size_t)2 * ML * TS * np;
+  double* myS = wcol + (size_t)warp * 2 * TS * np;
+  double* myL = myS + TS * np;
+
+  for (int64_t t = blockIdx.x; t < p.n_items; t += gridDim.x) {
+    const int a = p.f1[t], b = p.f2[t];
+    const int L1 = p.len[a], L2 = p.len[b];
+    if (L1 <= 0 || L2 <= 0) continue;
+    double c = lya_cos12(p.ux[a], p.uy[a], p.uz[a], p.ux[b], p.uy[b], p.uz[b], p.cos_variant);
+    c = fmin(1.0, fmax(-1.0, c));
+    const double ch = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(1.0, c)));
+    const double sh = __dsqrt_rn(__dmul_rn(0.5, __dsub_rn(1.0, c)));
+    const double om1 = p.omega[a], om2 = p.omega[b];
+    const double io1 = p.odl2[a] > 0.0 ? 1.0 / p.odl2[a] : 0.0;
+    const double io2 = p.odl2[b] > 0.0 ? 1.0 / p.odl2[b] : 0.0;
+    const bool srt = p.sorted[a] && p.sorted[b];
+    const int64_t A0 = p.pstart[a], B0 = p.pstart[b];
+    for (int k = tid; k < L1; k += DT) {
+      const double4 q = p.pix8[A0 + k];
+      sd[k] = q.x; sw[k] = q.y; sl[k] = p.dl[A0 + k];
+    }
+    for (int k = tid; k < L2; k += DT) {
+      const double4 q = p.pix8[B0 + k];
+      sd[ML + k] = q.x; sw[ML + k] = q.y; sl[ML + k] = p.dl[B0 + k];
+    }
+    if (tid == 0) { s_T0 = INT_MAX; s_T1 = -1; s_maxspan = 0; }
+    __syncthreads();
+
+    // ---- columns, one warp per pixel: side 0 = f1 pixels (partners in f2),
+    // side 1 = f2 pixels (partners in f1); built in shared memory with the
+    // lanes over the partners, then stored to the CTA's scratch
+    for (int side = 0; side < 2; ++side) {
+      const int Lm = side == 0 ? L1 : L2, Lo = side == 0 ? L2 : L1;
+      const double* dm = sd + side * ML;
+      const double* dO = sd + (1 - side) * ML;
+      const double* wO = sw + (1 - side) * ML;
+      const double* lO = sl + (1 - side) * ML;
+      double* cS = colS + (size_t)side * ML * TS * np;
+      double* cL = colL + (size_t)side * ML * TS * np;
+      for (int m = warp; m < Lm; m += NW) {
+        const double d = dm[m];
+        int jlo = 0, jhi = Lo;
+        if (srt) {   // partners with |d - d'| ch <= rpmax and (d + d') sh <= rtmax (+ margin)
+          const double reach = ch > 0.0 ? ((double)np + 1e-3) / (ch * p.binner_rp) : 1e300;
+          const double rt_reach = sh > 0.0 ? ((double)nt + 1e-3) / (sh * p.binner_rt) : 1e300;
+          const double tl = d - reach - 1e-6 * fabs(d) - 1e-6;
+          const double th = fmin(d + reach, rt_reach - d) + 1e-6 * fabs(d) + 1e-6;
+          int x = 0, y = Lo;
+          while (x < y) { const int q = (x + y) >> 1; if (dO[q] > tl) y = q; else x = q + 1; }
+          jlo = x;
+          y = Lo;
+          while (x < y) { const int q = (x + y) >> 1; if (dO[q] < th) x = q + 1; else y = q; }
+          jhi = x;
+        }
+        int lo = INT_MAX, hi = -1;
+        for (int o = jlo + lane; o < jhi; o += 32) {
+          const int A = side == 0 ? pair_bin(d, dO[o], ch, sh, p) : pair_bin(dO[o], d, ch, sh, p);
+          if (A >= 0) { const int bt = A % nt; lo = min(lo, bt); hi = max(hi, bt); }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+          hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        int sp = hi >= lo ? hi - lo + 1 : 0;
+        if (sp > TS) {
+          if (lane == 0) atomicAdd(p.err, 1ull);
+          sp = 0;
+        }
+        if (lane == 0) {
+          tlo[side * ML + m] = lo;
+          span[side * ML + m] = sp;
+        }
+        if (sp > 0) {
+          for (int q = lane; q < sp * np; q += 32) { myS[q] = 0.0; myL[q] = 0.0; }
+          __syncwarp();
+          for (int o = jlo + lane; o < jhi; o += 32) {
+            const int A = side == 0 ? pair_bin(d, dO[o], ch, sh, p) : pair_bin(dO[o], d, ch, sh, p);
+            if (A >= 0) {
+              const int bp = A / nt, bt = A - bp * nt;
+              const int q = (bt - lo) * np + bp;
+              atomicAdd(&myS[q], wO[o]);
+              atomicAdd(&myL[q], wO[o] * lO[o]);
+            }
+          }
+          __syncwarp();
+          double* rs = cS + (size_t)m * TS * np;
+          double* rl = cL + (size_t)m * TS * np;
+          for (int q = lane; q < sp * np; q += 32) { rs[q] = myS[q]; rl[q] = myL[q]; }
+          if (lane == 0) {
+            atomicMin(&s_T0, lo);
+            atomicMax(&s_T1, lo + sp - 1);
+            atomicMax(&s_maxspan, sp);
+          }
+          __syncwarp();
+        }
+      }
+    }
+    __syncthreads();
+    const int T0 = s_T0, T1 = s_T1, maxspan = s_maxspan;
+    if (T1 < T0) {   // no pixel pair in range
+      __syncthreads();
+      continue;
+    }
+    const int nT = T1 - T0 + 1;
+    // ---- pixels per rt bin: tlist[tcount[t-T0] ..] = (side << 16 | pixel) whose span covers t
+    for (int k = tid; k <= nT; k += DT) tcount[k] = 0;
+    __syncthreads();
+    for (int side = 0; side < 2; ++side) {
+      const int Lm = side == 0 ? L1 : L2;
+      for (int m = tid; m < Lm; m += DT)
+        for (int s = 0; s < span[side * ML + m]; ++s) atomicAdd(&tcount[tlo[side * ML + m] + s - T0 + 1], 1);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 1; k <= nT; ++k) tcount[k] += tcount[k - 1];
+      for (int k = 0; k < nT; ++k) tfill[k] = tcount[k];
+    }
+    __syncthreads();
+    for (int side = 0; side < 2; ++side) {
+      const int Lm = side == 0 ? L1 : L2;
+      for (int m = tid; m < Lm; m += DT)
+        for (int s = 0; s < span[side * ML + m]; ++s) {
+          const int pos = atomicAdd(&tfill[tlo[side * ML + m] + s - T0], 1);
+          tlist[pos] = (side << 16) | m;
+        }
+    }
+    __syncthreads();
+
+    // ---- moments of the touched bins (side 0 columns): entry e = (bp, t - T0)
+    const int ne = np * nT;
+    for (int e = tid; e < ne; e += DT) {
+      const int bp = e % np, tt = e / np, tb = T0 + tt;
+      double m0 = 0.0, mi = 0.0, mj = 0.0, mij = 0.0;
+      for (int q = tcount[tt]; q < tcount[tt + 1]; ++q) {
+        const int pk = tlist[q];
+        if ((pk >> 16) != 0) continue;
+        const int i = pk & 0xffff;
+        const size_t off = ((size_t)i * TS + (tb - tlo[i])) * np + bp;
+        const double s = colS[off], l = colL[off];
+        const double wi = sw[i], wli = sw[i] * sl[i];
+        m0 += wi * s; mj += wi * l; mi += wli * s; mij += wli * l;
+      }
+      mom[0 * nb + e] = m0; mom[1 * nb + e] = mi; mom[2 * nb + e] = mj; mom[3 * nb + e] = mij;
+    }
+    if (tid == 0) s_nnz = 0;
+    __syncthreads();
+    for (int e = tid; e < ne; e += DT) {
+      const double m0 = mom[e];
+      if (m0 != 0.0 || mom[nb + e] != 0.0 || mom[2 * nb + e] != 0.0 || mom[3 * nb + e] != 0.0) {
+        const int A = (e % np) * nt + T0 + e / np;
+        if (m0 != 0.0) {
+          atomicAdd(&p.W[A], m0);
+          atomicAdd(&p.D[(size_t)A * nb + A], m0);
+        }
+        nzlist[atomicAdd(&s_nnz, 1)] = e;
+      }
+    }
+    __syncthreads();
+    // ---- rank-4 part over touched bins
+    const int nnz = s_nnz;
+    const double cA = 1.0 / (om1 * om2), cB = io2 / om1, cC = io1 / om2, cD = io1 * io2;
+    for (int64_t q = tid; q < (int64_t)nnz * nnz; q += DT) {
+      const int e1 = nzlist[q / nnz], e2 = nzlist[q % nnz];
+      const double v = mom[e1] * mom[e2] * cA + mom[2 * nb + e1] * mom[2 * nb + e2] * cB +
+                       mom[nb + e1] * mom[nb + e2] * cC + mom[3 * nb + e1] * mom[3 * nb + e2] * cD;
+      if (v != 0.0) {
+        const int A = (e1 % np) * nt + T0 + e1 / np;
+        const int B = (e2 % np) * nt + T0 + e2 / np;
+        atomicAdd(&p.D[(size_t)A * nb + B], v);
+      }
+    }
+    // ---- column products: blocks (t, u) of rt bins, 50 x 50 (rp x rp) entries each
+    for (int tt = 0; tt < nT; ++tt) {
+      for (int uu = max(0, tt - (maxspan - 1)); uu <= min(nT - 1, tt + (maxspan - 1)); ++uu) {
+        const int tb = T0 + tt, ub = T0 + uu;
+        for (int e = tid; e < np * np; e += DT) {
+          const int bp = e / np, bq = e - bp * np;
+          double g = 0.0;
+          for (int q = tcount[tt]; q < tcount[tt + 1]; ++q) {
+            const int pk = tlist[q];
+            const int side = pk >> 16, m = pk & 0xffff;
+            const int lo = tlo[side * ML + m], sp = span[side * ML + m];
+            if (ub < lo || ub >= lo + sp) continue;
+            const double* cS = colS + (size_t)side * ML * TS * np + (size_t)m * TS * np;
+            const double* cL = colL + (size_t)side * ML * TS * np + (size_t)m * TS * np;
+            const double wm = sw[side * ML + m];
+            const double kS = side == 0 ? wm / om2 : wm / om1;
+            const double kL = side == 0 ? wm * io2 : wm * io1;
+            g += kS * cS[(tb - lo) * np + bp] * cS[(ub - lo) * np + bq] +
+                 kL * cL[(tb - lo) * np + bp] * cL[(ub - lo) * np + bq];
+          }
+          if (g != 0.0) atomicAdd(&p.D[(size_t)(bp * nt + tb) * nb + (bq * nt + ub)], -g);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_dist_run: ctx is NULL");
+  if (!ctx->bins_set) return lya_fail(ctx, LYA_ERR_STATE, "lya_dist_run: call lya_set_bins first");
+  if (ctx->cat.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_dist_run: no forests uploaded");
+  if (!ctx->cat.has_dl || !ctx->cat.has_moments)
+    return lya_fail(ctx, LYA_ERR_STATE, "lya_dist_run: upload dl, omega and odl2 with the forests");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int np = ctx->np, nt = ctx->nt, nb = np * nt;
+  int max_len = 1;
+  for (int64_t f = 0; f < ctx->cat.n; ++f)
+    max_len = std::max<int>(max_len, (int)(ctx->h_start[f + 1] - ctx->h_start[f]));
+  if (max_len > 65535) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests longer than 65535 pixels");
+  const size_t smem = sizeof(double) * (6 * (size_t)max_len + 4 * (size_t)nb + (size_t)NW * 2 * TS * np) +
+                      sizeof(int) * (4 * (size_t)max_len + 2 * (nt + 1) + 2 * (size_t)max_len * TS + nb);
+  if (smem > 227 * 1024)
+    return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory", max_len, smem);
+  const int grid = ctx->num_sms;
+  double *d_D = nullptr, *d_W = nullptr, *col = nullptr;
+  unsigned long long* err = nullptr;
+  cudaError_t e = lya_alloc(&d_D, (size_t)nb * nb);
+  if (e == cudaSuccess) e = lya_alloc(&d_W, nb);
+  if (e == cudaSuccess) e = lya_alloc(&col, (size_t)grid * 2 * 2 * max_len * TS * np);
+  if (e == cudaSuccess) e = lya_alloc(&err, 1);
+  auto cleanup = [&]() { lya_free(d_D); lya_free(d_W); lya_free(col); lya_free(err); };
+  if (e != cudaSuccess) {
+    cleanup();
+    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_dist_run: device allocation failed");
+  }
+  cudaStream_t s = ctx->stream;
+  e = cudaMemsetAsync(d_D, 0, sizeof(double) * (size_t)nb * nb, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_W, 0, sizeof(double) * nb, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
+  if (e == cudaSuccess && ctx->wq.n_pairs > 0) {
+    DistParams p;
+    p.pix8 = ctx->cat.pix8; p.dl = ctx->cat.dl; p.pstart = ctx->cat.pstart; p.len = ctx->cat.len;
+    p.sorted = ctx->cat.sorted; p.ux = ctx->cat.ux; p.uy = ctx->cat.uy; p.uz = ctx->cat.uz;
+    p.omega = ctx->cat.omega; p.odl2 = ctx->cat.odl2; p.f1 = ctx->wq.f1; p.f2 = ctx->wq.f2;
+    p.n_items = ctx->wq.n_pairs; p.max_len = max_len;
+    p.binner_rp = (double)np / ctx->rpmax; p.binner_rt = (double)nt / ctx->rtmax;
+    p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant;
+    p.col = col; p.D = d_D; p.W = d_W; p.err = err;
+    e = cudaFuncSetAttribute(k_dist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+      k_dist<<<grid, DT, smem, s>>>(p);
+      ctx->launches++;
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
+  unsigned long long nerr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nerr, err, sizeof(nerr), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && D) e = cudaMemcpyAsync(D, d_D, sizeof(double) * (size_t)nb * nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && W) e = cudaMemcpyAsync(W, d_W, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  cleanup();
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_dist_run: %s", cudaGetErrorString(e));
+  ctx->last.kernel_ms = ms;
+  if (nerr) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: %llu pixels pair into more than %d rt bins", nerr, TS);
+  return LYA_OK;
+}

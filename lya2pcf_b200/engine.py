@@ -167,6 +167,14 @@ class PairEngine:
             dw = np.ascontiguousarray(dw, dtype=np.float64)
             self._check(self.lib.lya_update_weights(self.ctx, N.ptr(w), N.ptr(dw), 0))
 
+    def distortion(self):
+        """Distortion numerator D[nb, nb] and bin weights W[nb] over the work
+        queue (FP64).  The normalised matrix of ``distortion.py`` is D / W[:, None]."""
+        D = np.zeros((self.nb, self.nb), dtype=np.float64)
+        W = np.zeros(self.nb, dtype=np.float64)
+        self._check(self.lib.lya_dist_run(self.ctx, N.ptr(D), N.ptr(W)))
+        return D, W
+
     def stats(self):
         st = N.Stats()
         self._check(self.lib.lya_stats(self.ctx, C.byref(st)))

@@ -454,7 +454,10 @@ int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const
     int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
     double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
     double chh = sqrt(0.5 * (1. + cos12)), shh = sqrt(0.5 * (1. - cos12));
-    double om1 = F->omega[a], om2 = F->omega[b], o21 = F->odl2[a], o22 = F->odl2[b];
+    /* 1/sum(w) and 1/sum(w dl^2); a forest whose dl are all 0 (e.g. one pixel)
+     * has no slope to project out, its slope terms are 0 instead of 0/0 */
+    double om1 = F->omega[a], om2 = F->omega[b];
+    double io21 = F->odl2[a] > 0.0 ? 1.0 / F->odl2[a] : 0.0, io22 = F->odl2[b] > 0.0 ? 1.0 / F->odl2[b] : 0.0;
     memset(e12, 0, sizeof(double) * (size_t)nb * (size_t)l1);
     memset(e13, 0, sizeof(double) * (size_t)nb * (size_t)l1);
     memset(e21, 0, sizeof(double) * (size_t)nb * (size_t)l2);
@@ -476,12 +479,12 @@ int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const
         act[B] = 1;
         e12[(size_t)B * l1 + i] += wj / om2;
         e21[(size_t)B * l2 + j] += wi / om1;
-        e13[(size_t)B * l1 + i] += wj * lj / o22;
-        e31[(size_t)B * l2 + j] += wi * li / o21;
+        e13[(size_t)B * l1 + i] += wj * lj * io22;
+        e31[(size_t)B * l2 + j] += wi * li * io21;
         e22[B] += wi * wj / (om1 * om2);
-        e23[B] += wi * wj * lj / (o22 * om1);
-        e32[B] += wi * li * wj / (o21 * om2);
-        e33[B] += wi * li * wj * lj / (o21 * o22);
+        e23[B] += wi * wj * lj * io22 / om1;
+        e32[B] += wi * li * wj * io21 / om2;
+        e33[B] += wi * li * wj * lj * io21 * io22;
         WB[B] += wi * wj;
       }
     }
