@@ -47,8 +47,12 @@ typedef struct {
   int32_t blocks_per_sm;   /* 0 = default (1) */
   int32_t slot_begin;      /* restrict the run to pairs whose first forest's */
   int32_t slot_end;        /* slot is in [slot_begin, slot_end); 0,0 = all    */
-  int32_t variant;         /* diagonal walk: 0 = default (FP32: two diagonals per
-                              lane, FP64: one), 1 = one per lane, 2 = two */
+  int32_t variant;         /* diagonal walk: 0 = default (FP32: the lean walk --
+                              two diagonals per lane, bin tests on the FP32 pixel
+                              coordinates -- for pairs of sorted forests with
+                              0 <= dc < 1e6, walk 2 for the others; FP64: one
+                              diagonal per lane), 1 = one diagonal per lane,
+                              2 = two diagonals per lane, 3 = same as 0 */
 } lya_corr_opts;
 
 typedef struct {

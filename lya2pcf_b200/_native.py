@@ -16,6 +16,7 @@ LYA_OK = 0
 KERNEL_FP32_GUARDED = 0
 KERNEL_FP64_DIAGONAL = 1
 KERNEL_FP64_PLAIN = 2
+VARIANT_TWO_DIAGONALS = 2   # lya_corr_opts.variant: FP32 kernel without its lean walk
 NQ = 5
 Q_W, Q_DW, Q_RP, Q_RT, Q_Z = range(NQ)
 

@@ -123,9 +123,11 @@ __global__ void k_pack(int64_t n, const int64_t* __restrict__ start, const int64
                        int32_t* __restrict__ o_len, uint8_t* __restrict__ o_sorted) {
   for (int64_t f = blockIdx.x; f < n; f += gridDim.x) {
     const int64_t s = start[f], L = start[f + 1] - s, d = pstart[f];
-    int ok = 1;
+    int ok = 1, lean = 1;
     for (int64_t k = threadIdx.x; k < L; k += blockDim.x) {
       const double x = dc[s + k];
+      // the FP32 error bound of the lean walk assumes 0 <= dc < 1e6 Mpc/h
+      if (!(x >= 0.0 && x < LYA_LEAN_DC_MAX)) lean = 0;
       o_dc[d + k] = x;
       o_w[d + k] = w[s + k];
       o_dw[d + k] = dw[s + k];
@@ -139,9 +141,10 @@ __global__ void k_pack(int64_t n, const int64_t* __restrict__ start, const int64
       if (k + 1 < L && !(x <= dc[s + k + 1])) ok = 0;
     }
     ok = __syncthreads_and(ok);
+    lean = __syncthreads_and(lean);
     if (threadIdx.x == 0) {
       o_len[f] = (int32_t)L;
-      o_sorted[f] = (uint8_t)ok;
+      o_sorted[f] = (uint8_t)(ok ? (lean ? (LYA_SORTED | LYA_LEAN) : LYA_SORTED) : 0);
     }
     __syncthreads();
   }

@@ -80,8 +80,16 @@ struct LaneStats {
 // Shared-memory histogram of the slot being accumulated.
 struct SmemHist {
   double* q;                  // [LYA_NQ][nb]
-  unsigned long long* n;      // [nb]
+  unsigned int* n;            // [nb] pair counts (native 32-bit shared atomics)
+  unsigned long long* gc;     // [nb] global counts of the slot being accumulated
 };
+
+// Count n more pairs in bin b: a 32-bit shared counter whose wrap-around is
+// carried into the slot's global 64-bit count, so counts stay exact.
+__device__ __forceinline__ void count_pairs(const SmemHist& h, int b, unsigned int n) {
+  const unsigned int old = atomicAdd(&h.n[b], n);
+  if (old > 0xffffffffu - n) atomicAdd(&h.gc[b], 1ull << 32);
+}
 
 __device__ __forceinline__ void pair_half_angles(const CorrParams& p, int a, int b, double& ch, double& sh) {
   double c = lya_cos12(p.ux[a], p.uy[a], p.uz[a], p.ux[b], p.uy[b], p.uz[b], p.cos_variant);
@@ -166,7 +174,7 @@ __device__ __forceinline__ void drain(Rec* buf, int cnt, const SmemHist& h, int 
     atomicAdd(&h.q[2 * nb + r.bin], (double)r.ax);
     atomicAdd(&h.q[3 * nb + r.bin], (double)r.ay);
     atomicAdd(&h.q[4 * nb + r.bin], (double)r.az);
-    atomicAdd(&h.n[r.bin], (unsigned long long)r.n);
+    count_pairs(h, r.bin, (unsigned int)r.n);
   }
   __syncwarp();
 }
@@ -639,6 +647,364 @@ __device__ void item_diag2(const CorrParams& p, int64_t t, const SmemHist& h, ty
   }
 }
 
+// ------------------------------------------------------------------ lean walk (FP32, both forests lean)
+// Same lane layout as item_diag2 (lane l: diagonals m = mg + 2l and m + 1 at
+// f1 pixel i = base + k - l), for forest pairs whose dc are sorted, finite and
+// in [0, LYA_LEAN_DC_MAX).  The bin tests run on the FP32 pixel coordinates
+// themselves:
+//   e = |(hi1 - hi2) + (lo1 - lo2)|  ~ |dc1 - dc2|,    s = hi1 + hi2  ~ dc1 + dc2
+// against per-forest-pair FP32 threshold tables built with directed rounding:
+//   e >= tlo[b]  =>  X64 >= b,   e < thi[b]  =>  X64 < b + 1,   e >= tout => X64 >= np
+// (X64 the reference's FP64 bin coordinate of rp; likewise slo, shi, scut for
+// rt and s), tlo[b] = RU((b + g)/cx), thi[b] = RD((b + 1 - g)/cx), cx = ch*np/rpmax,
+// g the guard in bin units.  |e - |dc1-dc2|| <= 2^-23 |dc1-dc2| + 2^-45 (dc1+dc2)
+// and |s - (dc1+dc2)| <= 2^-23 (dc1+dc2) (|lo| <= 2^-24 hi), so every
+// accepted bin is the FP64 formula's bin when g is at least
+// (n+1)(2^-23 + 2^-50)*1.1 + 1e-7 bins (2.7e-5 Mpc/h for 50 bins of 4 Mpc/h),
+// below the bound the host already enforces for the other walks.
+// s is non-decreasing along a diagonal of two sorted forests, so the rt test is
+// one-sided and a diagonal ends for good once s >= scut.  A run's state is its
+// bin and its interval [tlo, thi) x [.., shi); a pair outside the interval is
+// an event: the run is closed (record), shifted to the adjacent rp or rt bin
+// when the pair lies inside that bin's interval, otherwise classified again
+// (tables, or the reference FP64 formula inside the guard band).  Sums run over
+// e and s and are scaled to bin units (x = e*cx, y = s*cy) when a run is
+// recorded.  Each lane's first run is classified before the walk, so ragged
+// diagonal starts cost no event; one vote covers two steps (four pairs).
+// Per-warp state of the forest pair being walked, in shared memory (read on
+// the rare paths only, so the walk's registers hold just the runs, the sums and
+// the pixels); the threshold tables follow it: tlo[np], thi[np], slo[nt], shi[nt].
+struct __align__(16) LeanCtl {
+  double ch, sh;
+  const double4* d1;     // FP64 pixels of f1 (i = 0)
+  const double4* d2;     // FP64 pixels of f2 (j = 0)
+  float tout, scut;      // e >= tout: beyond rpmax;  s >= scut: beyond rtmax
+  float cxf, cyf;        // FP32 copies of cx, cy: candidate bins and record scaling
+  int base, mg;          // current pass: f1 pixel i = base + k - lane, f2 pixel j = base + mg + lane + k
+  int pad0, pad1;
+};
+constexpr int LEAN_CTL_FLOATS = (int)(sizeof(LeanCtl) / sizeof(float));
+// floats per warp: the state and the tables, rounded to keep the next warp's state 16-byte aligned
+__host__ __device__ __forceinline__ int lean_ctl_stride(int np, int nt) {
+  return LEAN_CTL_FLOATS + ((2 * (np + nt) + 3) & ~3);
+}
+
+__device__ __forceinline__ float* lean_tab(LeanCtl* c) { return reinterpret_cast<float*>(c + 1); }
+
+struct LeanRun {
+  int bx, by, k0;
+  float tlo, thi, shi;
+};
+
+struct LeanAcc {
+  float aw, adw, ae, as, az;
+  __device__ __forceinline__ void zero() { aw = adw = ae = as = az = 0.f; }
+  __device__ __forceinline__ void add(const float4& a, float za, const float4& b, float zb, float e, float s) {
+    const float w12 = a.z * b.z;
+    aw += w12;
+    adw = fmaf(a.w, b.w, adw);
+    ae = fmaf(w12, e, ae);
+    as = fmaf(w12, s, as);
+    az = fmaf(w12, za + zb, az);
+  }
+};
+
+__device__ __forceinline__ float lean_e(const float4& a, const float4& b) { return fabsf((a.x - b.x) + (a.y - b.y)); }
+__device__ __forceinline__ float lean_s(const float4& a, const float4& b) { return a.x + b.x; }
+
+// true when the pair (e, s) lies outside the run's interval (NaN-safe form)
+__device__ __forceinline__ bool lean_out(const LeanRun& r, float e, float s) {
+  return !(e >= r.tlo) || !(e < r.thi) || !(s < r.shi);
+}
+
+// Per-forest-pair state and threshold tables of one warp.
+__device__ __forceinline__ void lean_setup(LeanCtl* c, double ch, double sh, const double4* d1, const double4* d2,
+                                           const CorrParams& p) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();   // every lane is done with the previous forest pair's state
+  const double cx = __dmul_rn(ch, p.binner_rp), cy = __dmul_rn(sh, p.binner_rt);
+  const double gx = (double)p.gx, gy = (double)p.gy;
+  float* tlo = lean_tab(c);
+  float* thi = tlo + p.np;
+  float* slo = thi + p.np;
+  float* shi = slo + p.nt;
+  for (int b = lane; b < p.np; b += 32) {
+    tlo[b] = b == 0 ? -1.0f : __double2float_ru(__ddiv_ru((double)b + gx, cx));
+    thi[b] = __double2float_rd(__ddiv_rd((double)(b + 1) - gx, cx));
+  }
+  for (int b = lane; b < p.nt; b += 32) {
+    slo[b] = b == 0 ? -1.0f : __double2float_ru(__ddiv_ru((double)b + gy, cy));
+    shi[b] = __double2float_rd(__ddiv_rd((double)(b + 1) - gy, cy));
+  }
+  if (lane == 0) {
+    c->ch = ch; c->sh = sh; c->d1 = d1; c->d2 = d2;
+    c->tout = __double2float_ru(__ddiv_ru((double)p.np + gx, cx));
+    c->scut = __double2float_ru(__ddiv_ru((double)p.nt + gy, cy));
+    c->cxf = __double2float_rn(cx);
+    c->cyf = __double2float_rn(cy);
+  }
+  __syncwarp();
+}
+
+// Full classification of the pair (e, s) at step k of diagonal dm (0: a, 1: b)
+// of this lane, which starts a run.  Sets the lane's diagonal end kend = k when
+// the diagonal is past rtmax.
+__device__ __forceinline__ void lean_classify(const CorrParams& p, const LeanCtl* c, LeanRun& r, float e, float s,
+                                           int& kend, int k, int dm, LaneStats& st) {
+  const float INF = __int_as_float(0x7f800000);
+  const float* tlo = lean_tab(const_cast<LeanCtl*>(c));
+  const float* thi = tlo + p.np;
+  const float* slo = thi + p.np;
+  const float* shi = slo + p.nt;
+  const float scut = c->scut, tout = c->tout;
+  if (!(s < scut)) {   // past rtmax for good (s only grows): the diagonal is done
+    kend = k;
+    r.bx = -1; r.by = -1; r.tlo = -INF; r.thi = INF; r.shi = INF;
+    return;
+  }
+  if (e >= tout) {     // beyond rpmax; |dc1-dc2| may shrink again
+    r.bx = -1; r.by = -1; r.tlo = tout; r.thi = INF; r.shi = scut;
+    return;
+  }
+  const int cbx = min((int)(e * c->cxf), p.np - 1);
+  const int cby = min((int)(s * c->cyf), p.nt - 1);
+  const float tl = tlo[cbx], th = thi[cbx], sl = slo[cby], su = shi[cby];
+  if (e >= tl && e < th && s >= sl && s < su) {
+    r.bx = cbx; r.by = cby; r.tlo = tl; r.thi = th; r.shi = su;
+    return;
+  }
+  // guard band (or an FP32 candidate one bin off): the reference FP64 formula
+  // decides this pair; the empty interval re-examines the next one
+  const int lane = threadIdx.x & 31;
+  const int i = c->base - lane + k, j = c->base + c->mg + lane + k + dm;
+  double rp, rt;
+  const int b = bin_fp64(p, c->d1[i].x, c->d2[j].x, c->ch, c->sh, rp, rt);
+  if (b >= 0) { r.bx = b / p.nt; r.by = b - r.bx * p.nt; } else { r.bx = -1; r.by = -1; }
+  r.tlo = INF; r.thi = -INF; r.shi = -INF;
+  st.recheck++;
+}
+
+// Move the run to the adjacent bin the pair (e, s) lies in, when one rp or one
+// rt edge was crossed; false when a full classification is needed.
+__device__ __forceinline__ bool lean_shift(const CorrParams& p, const LeanCtl* c, LeanRun& r, float e, float s) {
+  const float INF = __int_as_float(0x7f800000);
+  if (r.bx < 0) return false;
+  const bool xo = !(e >= r.tlo) || !(e < r.thi);
+  const bool yo = !(s < r.shi);
+  if (xo == yo) return false;
+  const float* tlo = lean_tab(const_cast<LeanCtl*>(c));
+  if (xo) {
+    const int nbx = e >= r.thi ? r.bx + 1 : r.bx - 1;
+    if (nbx >= p.np) {
+      const float tout = c->tout;
+      if (!(e >= tout)) return false;
+      r.bx = -1; r.by = -1; r.tlo = tout; r.thi = INF; r.shi = c->scut;
+      return true;
+    }
+    if (nbx < 0) return false;
+    const float tl = tlo[nbx], th = tlo[p.np + nbx];
+    if (!(e >= tl && e < th)) return false;
+    r.bx = nbx; r.tlo = tl; r.thi = th;
+    return true;
+  }
+  const int nby = r.by + 1;
+  if (nby >= p.nt) return false;
+  const float sl = tlo[2 * p.np + nby], su = tlo[2 * p.np + p.nt + nby];
+  if (!(s >= sl && s < su)) return false;
+  r.by = nby; r.shi = su;
+  return true;
+}
+
+struct LeanWalk {
+  const CorrParams& p;
+  LeanCtl* c;
+  const SmemHist& h;
+  RecF32* buf;
+  int& cnt;
+  LaneStats& st;
+  int ka_beg, kb_beg, ka_end, kb_end;
+  int kall;   // last step any lane of the warp still walks (exclusive)
+  LeanRun ra, rb;
+  LeanAcc acca, accb;
+
+  __device__ __forceinline__ void record(bool w, const LeanRun& r, const LeanAcc& acc, int k, unsigned bal, int pos) {
+    if (w) {
+      const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+      RecF32 rec;
+      rec.bin = r.bx * p.nt + r.by; rec.n = k - r.k0;
+      rec.aw = acc.aw; rec.adw = acc.adw; rec.ax = acc.ae * c->cxf; rec.ay = acc.as * c->cyf; rec.az = acc.az;
+      rec.pad = 0.f;
+      buf[pos + __popc(bal & lt)] = rec;
+    }
+  }
+
+  // close both runs at step ka / kb for the lanes in live_*; records for in-range runs
+  __device__ __forceinline__ void close(bool live_a, bool live_b, int ka, int kb) {
+    const bool wa = live_a && ra.bx >= 0 && ka > ra.k0;
+    const bool wb = live_b && rb.bx >= 0 && kb > rb.k0;
+    const unsigned bala = __ballot_sync(FULL, wa), balb = __ballot_sync(FULL, wb);
+    record(wa, ra, acca, ka, bala, cnt);
+    record(wb, rb, accb, kb, balb, cnt + __popc(bala));
+    cnt += __popc(bala) + __popc(balb);
+    if (live_a) { acca.zero(); ra.k0 = ka; }
+    if (live_b) { accb.zero(); rb.k0 = kb; }
+    if (cnt > REC - 64) {
+      drain(buf, cnt, h, p.nb, st);
+      cnt = 0;
+    }
+  }
+
+  // One step with event handling: pair a = (q1, qa), pair b = (q1, qb).
+  __device__ __forceinline__ void slow_step(int k, const float4& q1, float z1, const float4& qa, float za,
+                                            const float4& qb, float zb) {
+    const float ea = lean_e(q1, qa), sa = lean_s(q1, qa);
+    const float eb = lean_e(q1, qb), sb = lean_s(q1, qb);
+    bool act_a = k >= ka_beg && k < ka_end;
+    bool act_b = k >= kb_beg && k < kb_end;
+    const bool exa = act_a && lean_out(ra, ea, sa);
+    const bool exb = act_b && lean_out(rb, eb, sb);
+    if (__any_sync(FULL, exa || exb)) {
+      const bool wa = exa && ra.bx >= 0 && k > ra.k0;
+      const bool wb = exb && rb.bx >= 0 && k > rb.k0;
+      const unsigned bala = __ballot_sync(FULL, wa), balb = __ballot_sync(FULL, wb);
+      record(wa, ra, acca, k, bala, cnt);
+      record(wb, rb, accb, k, balb, cnt + __popc(bala));
+      cnt += __popc(bala) + __popc(balb);
+      const bool fa = exa && !lean_shift(p, c, ra, ea, sa);
+      const bool fb = exb && !lean_shift(p, c, rb, eb, sb);
+      if (exa) { acca.zero(); ra.k0 = k; }
+      if (exb) { accb.zero(); rb.k0 = k; }
+      if (__any_sync(FULL, fa || fb)) {
+        if (fa) lean_classify(p, c, ra, ea, sa, ka_end, k, 0, st);
+        if (fb) lean_classify(p, c, rb, eb, sb, kb_end, k, 1, st);
+        act_a = act_a && k < ka_end;
+        act_b = act_b && k < kb_end;
+        int ke = max(ka_end, kb_end);   // diagonals past rtmax shorten the walk
+        for (int o = 16; o > 0; o >>= 1) ke = max(ke, __shfl_xor_sync(FULL, ke, o));
+        kall = min(kall, ke);
+      }
+      if (cnt > REC - 64) {
+        drain(buf, cnt, h, p.nb, st);
+        cnt = 0;
+      }
+    }
+    if (act_a) acca.add(q1, z1, qa, za, ea, sa);
+    if (act_b) accb.add(q1, z1, qb, zb, eb, sb);
+  }
+};
+
+__device__ void item_lean(const CorrParams& p, int64_t t, const SmemHist& h, RecF32* buf, LeanCtl* ctl, int& cnt,
+                          LaneStats& st) {
+  const int lane = threadIdx.x & 31;
+  const int fa = p.f1[t], fb = p.f2[t];
+  const int L1 = p.len[fa], L2 = p.len[fb];
+  if (L1 <= 0 || L2 <= 0) return;
+  const int64_t a = p.pstart[fa], b = p.pstart[fb];
+  int m_lo, m_hi;
+  {
+    double ch, sh;
+    pair_half_angles(p, fa, fb, ch, sh);
+    lean_setup(ctl, ch, sh, p.pix8 + a, p.pix8 + b, p);
+    const float4* __restrict__ P1 = p.pix4 + a;
+    const float4* __restrict__ P2 = p.pix4 + b;
+    const double slack = 2.0 * p.gx;
+    const double rp_reach = ch > 0.0 ? ((double)p.np + slack) / (ch * p.binner_rp) : 1e300;
+    const double rt_reach = sh > 0.0 ? ((double)p.nt + slack) / (sh * p.binner_rt) : 1e300;
+    diagonal_band(L1, L2, P1, [&](int j) { return P2[j].x; }, rp_reach, rt_reach, m_lo, m_hi);
+  }
+  LeanWalk W{p, ctl, h, buf, cnt, st};
+  const int cap = p.run_cap;   // power of two, even
+  for (int mg = m_lo; mg <= m_hi; mg += 64) {
+    const int ma = mg + 2 * lane, mb = ma + 1;
+    const int ia_lo = max(0, -ma), ia_hi = (ma <= m_hi) ? min(L1, L2 - ma) : ia_lo;
+    const int ib_lo = max(0, -mb), ib_hi = (mb <= m_hi) ? min(L1, L2 - mb) : ib_lo;
+    const bool ne_a = ia_lo < ia_hi, ne_b = ib_lo < ib_hi;
+    int base = min(ne_a ? ia_lo + lane : INT_MAX, ne_b ? ib_lo + lane : INT_MAX);
+    for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
+    if (base == INT_MAX) continue;
+    W.ka_beg = ne_a ? ia_lo + lane - base : 0;
+    W.kb_beg = ne_b ? ib_lo + lane - base : 0;
+    W.ka_end = ne_a ? ia_hi + lane - base : 0;
+    W.kb_end = ne_b ? ib_hi + lane - base : 0;
+    int k_end = max(W.ka_end, W.kb_end);
+    for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
+    W.kall = k_end;
+    __syncwarp();
+    if (lane == 0) { ctl->base = base; ctl->mg = mg; }
+    __syncwarp();
+    const int ioff = base - lane;        // i = ioff + k    (>= -31)
+    const int joff = base + mg + lane;   // j_a = joff + k  (>= -31), j_b = j_a + 1
+    const float4* __restrict__ A1 = p.pix4 + a + ioff;
+    const float* __restrict__ Z1 = p.z32 + a + ioff;
+    const float4* __restrict__ A2 = p.pix4 + b + joff;
+    const float* __restrict__ Z2 = p.z32 + b + joff;
+    // each lane's first run, classified before the walk
+    W.acca.zero();
+    W.accb.zero();
+    {
+      const float INF = __int_as_float(0x7f800000);
+      W.ra.bx = -1; W.ra.by = -1; W.ra.tlo = INF; W.ra.thi = -INF; W.ra.shi = -INF;
+      W.rb = W.ra;
+      W.ra.k0 = W.ka_beg;
+      W.rb.k0 = W.kb_beg;
+      if (ne_a) {
+        const int k = W.ka_beg;
+        const float4 u = A1[k], v = A2[k];
+        lean_classify(p, ctl, W.ra, lean_e(u, v), lean_s(u, v), W.ka_end, k, 0, st);
+      }
+      if (ne_b) {
+        const int k = W.kb_beg;
+        const float4 u = A1[k], v = A2[k + 1];
+        lean_classify(p, ctl, W.rb, lean_e(u, v), lean_s(u, v), W.kb_end, k, 1, st);
+      }
+      int ke = max(W.ka_end, W.kb_end);   // first runs past rtmax
+      for (int o = 16; o > 0; o >>= 1) ke = max(ke, __shfl_xor_sync(FULL, ke, o));
+      W.kall = min(W.kall, ke);
+    }
+    // steps k, k+1 per iteration: f1 pixels q1a (k), q1b (k+1); f2 pixels
+    // q2x (k), q2y (k+1), q2z (k+2).  Pairs: a@k = (q1a, q2x), b@k = (q1a, q2y),
+    // a@k+1 = (q1b, q2y), b@k+1 = (q1b, q2z).
+    float4 q1a = A1[0], q2x = A2[0], q2y = A2[1];
+    float z1a = Z1[0], z2x = Z2[0], z2y = Z2[1];
+    int k = 0;
+    for (; k < W.kall; k += 2) {
+      const float4 q1b = A1[k + 1], q2z = A2[k + 2];
+      const float z1b = Z1[k + 1], z2z = Z2[k + 2];
+      const float e0a = lean_e(q1a, q2x), s0a = lean_s(q1a, q2x);
+      const float e0b = lean_e(q1a, q2y), s0b = lean_s(q1a, q2y);
+      const float e1a = lean_e(q1b, q2y), s1a = lean_s(q1b, q2y);
+      const float e1b = lean_e(q1b, q2z), s1b = lean_s(q1b, q2z);
+      const bool a0 = k >= W.ka_beg && k < W.ka_end, b0 = k >= W.kb_beg && k < W.kb_end;
+      const bool a1 = k + 1 >= W.ka_beg && k + 1 < W.ka_end, b1 = k + 1 >= W.kb_beg && k + 1 < W.kb_end;
+      const bool ev = (a0 && lean_out(W.ra, e0a, s0a)) || (b0 && lean_out(W.rb, e0b, s0b)) ||
+                      (a1 && lean_out(W.ra, e1a, s1a)) || (b1 && lean_out(W.rb, e1b, s1b));
+      if (__any_sync(FULL, ev)) {
+        W.slow_step(k, q1a, z1a, q2x, z2x, q2y, z2y);
+        W.slow_step(k + 1, q1b, z1b, q2y, z2y, q2z, z2z);
+      } else {
+        if (a0) W.acca.add(q1a, z1a, q2x, z2x, e0a, s0a);
+        if (b0) W.accb.add(q1a, z1a, q2y, z2y, e0b, s0b);
+        if (a1) W.acca.add(q1b, z1b, q2y, z2y, e1a, s1a);
+        if (b1) W.accb.add(q1b, z1b, q2z, z2z, e1b, s1b);
+      }
+      q1a = A1[k + 2];
+      z1a = Z1[k + 2];
+      q2x = q2z;
+      z2x = z2z;
+      q2y = A2[k + 3];
+      z2y = Z2[k + 3];
+      // registers now hold f1[k+2], f2[k+2], f2[k+3]: the next iteration's pixels
+      if (((k + 2) & (cap - 1)) == 0) {   // bound the length of a register sum
+        W.close(k + 1 >= W.ka_beg && k + 1 < W.ka_end, k + 1 >= W.kb_beg && k + 1 < W.kb_end, k + 2, k + 2);
+        if (__all_sync(FULL, k + 2 >= W.ka_end && k + 2 >= W.kb_end)) { k += 2; break; }
+      }
+    }
+    const int kfa = min(W.ka_end, k_end), kfb = min(W.kb_end, k_end);
+    st.evaluated += (unsigned long long)(max(0, kfa - W.ka_beg) + max(0, kfb - W.kb_beg));
+    W.close(true, true, max(kfa, W.ra.k0), max(kfb, W.rb.k0));
+  }
+}
+
 // ------------------------------------------------------------------ FP64 plain (every pixel pair)
 __device__ void item_plain(const CorrParams& p, int64_t t, const SmemHist& h, LaneStats& st) {
   const int lane = threadIdx.x & 31;
@@ -662,7 +1028,7 @@ __device__ void item_plain(const CorrParams& p, int64_t t, const SmemHist& h, La
         atomicAdd(&h.q[2 * p.nb + k], __dmul_rn(w12, rp));
         atomicAdd(&h.q[3 * p.nb + k], __dmul_rn(w12, rt));
         atomicAdd(&h.q[4 * p.nb + k], __dmul_rn(w12, __dadd_rn(q1.w, q2.w)));
-        atomicAdd(&h.n[k], 1ull);
+        count_pairs(h, k, 1u);
         st.inrange++;
       }
     }
@@ -692,16 +1058,21 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
   const int nb = p.nb;
   SmemHist h;
   h.q = reinterpret_cast<double*>(smem);
-  h.n = reinterpret_cast<unsigned long long*>(h.q + LYA_NQ * nb);
-  unsigned char* bufs = reinterpret_cast<unsigned char*>(h.n + nb);
+  h.n = reinterpret_cast<unsigned int*>(h.q + LYA_NQ * nb);
+  h.gc = nullptr;
+  // the count array keeps 8 bytes per bin so the record buffers stay 16-byte aligned
+  unsigned char* bufs = reinterpret_cast<unsigned char*>(h.q + LYA_NQ * nb) + (size_t)nb * sizeof(unsigned long long);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* mybuf = bufs + (size_t)warp * REC * rec_bytes<KIND>();
+  // lean walk: per-warp state and threshold tables after the record buffers
+  LeanCtl* myctl = reinterpret_cast<LeanCtl*>(reinterpret_cast<float*>(bufs + (size_t)WARPS * REC * rec_bytes<KIND>()) +
+                                              (size_t)warp * lean_ctl_stride(p.np, p.nt));
   __shared__ unsigned long long s_next;
   __shared__ long long s_seg_end;
   __shared__ int s_slot;
 
   for (int k = threadIdx.x; k < LYA_NQ * nb; k += blockDim.x) h.q[k] = 0.0;
-  for (int k = threadIdx.x; k < nb; k += blockDim.x) h.n[k] = 0ull;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) h.n[k] = 0u;
   LaneStats st;
   int cnt = 0;   // records pending in this warp's buffer (warp-uniform)
   const int64_t begin = p.cta_begin[blockIdx.x], end = p.cta_begin[blockIdx.x + 1];
@@ -722,6 +1093,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
     __syncthreads();
     const int64_t seg_end = s_seg_end;
     const int slot = s_slot;
+    h.gc = p.counts + (size_t)slot * nb;
     for (;;) {
       unsigned long long t = 0;
       if (lane == 0) t = atomicAdd(&s_next, 1ull);
@@ -729,6 +1101,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
       if ((int64_t)t >= seg_end) break;
       if (KIND == LYA_KERNEL_FP32_GUARDED) {
         if (p.variant == 1) item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+        else if (p.variant != 2 && (p.sorted[p.f1[t]] & p.sorted[p.f2[t]] & LYA_LEAN))
+          item_lean(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), myctl, cnt, st);
         else item_diag2<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
       } else if (KIND == LYA_KERNEL_FP64_DIAGONAL) {
         if (p.variant == 2) item_diag2<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
@@ -755,8 +1129,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
     }
     unsigned long long* gc = p.counts + (size_t)slot * nb;
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-      if (h.n[k]) atomicAdd(&gc[k], h.n[k]);
-      h.n[k] = 0ull;
+      if (h.n[k]) atomicAdd(&gc[k], (unsigned long long)h.n[k]);
+      h.n[k] = 0u;
     }
     __syncthreads();
     seg = seg_end;
@@ -780,7 +1154,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
 template <int KIND, int WARPS>
 cudaError_t launch_corr(const CorrParams& p, int nctas, int nb, cudaStream_t s) {
   const size_t smem = (size_t)nb * (LYA_NQ * sizeof(double) + sizeof(unsigned long long)) +
-                      (size_t)WARPS * REC * rec_bytes<KIND>();
+                      (size_t)WARPS * REC * rec_bytes<KIND>() +
+                      (KIND == LYA_KERNEL_FP32_GUARDED ? (size_t)WARPS * lean_ctl_stride(p.np, p.nt) * sizeof(float) : 0);
   cudaError_t e = cudaFuncSetAttribute(k_corr<KIND, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k_corr<KIND, WARPS><<<nctas, WARPS * 32, smem, s>>>(p);
@@ -965,7 +1340,11 @@ extern "C" int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts) {
   if (opts) o = *opts;
   if (o.kernel < 0 || o.kernel > 2) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: unknown kernel %d", o.kernel);
   if (o.blocks_per_sm < 0 || o.blocks_per_sm > 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: blocks_per_sm must be 0 or 1");
-  if (o.variant < 0 || o.variant > 2) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant must be 0, 1 or 2");
+  if (o.variant < 0 || o.variant > 3) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant must be 0, 1, 2 or 3");
+  if (o.variant == 3 && o.kernel != LYA_KERNEL_FP32_GUARDED)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant 3 (lean walk) exists for the FP32 kernel only");
+  if (o.kernel == LYA_KERNEL_FP32_GUARDED && (size_t)2 * (ctx->np + ctx->nt) > 1024)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: FP32 kernel needs np + nt <= 512 (threshold tables)");
   if (o.warps_per_block != 0 && o.warps_per_block != 16)
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: warps_per_block must be 0 or 16");
   if (o.slot_begin < 0 || o.slot_end < o.slot_begin || o.slot_end > ctx->cat.n_slots)

@@ -22,10 +22,17 @@
 // column of a pixel spans a few rt bins only, so the column products are
 // 50x50 dense blocks (rp x rp) per pair of rt bins.
 //
-// One CTA per forest pair (grid-stride).  Bins come from the reference FP64
-// formula.  Columns live in CTA-private global scratch (a thread owns a pixel,
-// no atomics), moments in shared memory; D (np*nt squared FP64, 50 MB for 50x50
-// bins, L2-resident) receives one atomic add per touched entry per forest pair.
+// One CTA per forest pair (dynamic queue).  Bins come from the reference FP64
+// formula.  Phase 1: the columns of every pixel (a warp per pixel, lanes over
+// its partners) go to CTA-private global scratch as dense [TS rt bins][np]
+// rows.  Phase 2: the 50x50 (rp x rp) blocks (t, u) of D over the pair's window
+// of rt bins, diagonal blocks first (they complete the moments of bin t, read
+// from the same staged rows).  A block whose rt bins are both spanned by some
+// pixel column gets the column products as a small dense FP64 GEMM: the rows
+// of the pixels covering t and u are staged in shared memory in chunks of CH
+// pixels and every thread accumulates a TR x TC register tile; the rank-4 and
+// diagonal terms are added to the tile, and each D entry of the window gets
+// one atomic add per forest pair (both (A, B) and (B, A): D is symmetric).
 // A forest whose sum w dl^2 is 0 has no slope to project out: its slope terms
 // are 0.
 #include <algorithm>
@@ -36,8 +43,12 @@
 namespace {
 
 constexpr int DT = 256;       // threads per CTA
-constexpr int TS = 6;         // rt bins a pixel column may span
+constexpr int TS = 8;         // rt bins a pixel column may span
 constexpr int NW = DT / 32;   // warps per CTA
+constexpr int CH = 32;        // pixels per staged chunk of a block
+constexpr int TR = 2, TC = 5; // register tile of a thread (rp rows x rp columns)
+constexpr int NP_MAX = 64;    // np of the tiled blocks: ceil(64/2)*ceil(64/5) = 416 tiles <= 2 per thread
+constexpr int TPT = 2;        // tiles per thread
 
 struct DistParams {
   const double4* __restrict__ pix8;   // (dc, w, dw, z)
@@ -56,10 +67,12 @@ struct DistParams {
   int max_len;
   double binner_rp, binner_rt;
   int np, nt, nb, cos_variant;
+  int npad;                // staged row length (>= np, covers every tile)
   double* col;             // scratch [grid][2 sides][max_len][TS][np] x {S, L}
   double* D;               // [nb][nb]
   double* W;               // [nb]
   unsigned long long* err; // [1] pixels whose column spans more than TS rt bins
+  unsigned long long* next;// [1] work queue counter
 };
 
 __device__ __forceinline__ int pair_bin(double d1, double d2, double ch, double sh, const DistParams& p) {
@@ -74,30 +87,38 @@ __device__ __forceinline__ int pair_bin(double d1, double d2, double ch, double 
 __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int ML = p.max_len;
-  const int np = p.np, nt = p.nt, nb = p.nb;
+  const int np = p.np, nt = p.nt, nb = p.nb, NPAD = p.npad;
   double* sd = reinterpret_cast<double*>(smem);          // [2][ML] dc
   double* sw = sd + 2 * ML;                              // [2][ML] w
   double* sl = sw + 2 * ML;                              // [2][ML] dl
-  double* mom = sl + 2 * ML;                             // [4][nb] moments of the touched bins
-  double* wcol = mom + 4 * nb;                           // [NW][2][TS*np] a warp's column being built
-  int* tlo = reinterpret_cast<int*>(wcol + NW * 2 * TS * np);   // [2][ML]
+  double* mom = sl + 2 * ML;                             // [4][nt][np] moments of the window's bins
+  double* stage = mom + 4 * nt * np;                     // [4][CH][NPAD] staged rows, or the column builders
+  const int stage_len = max(4 * CH * NPAD, NW * 2 * TS * np);
+  int* tlo = reinterpret_cast<int*>(stage + stage_len);  // [2][ML]
   int* span = tlo + 2 * ML;                              // [2][ML]
-  int* tcount = span + 2 * ML;                           // [nt + 1]
-  int* tfill = tcount + (nt + 1);                        // [nt + 1]
-  int* tlist = tfill + (nt + 1);                         // [2*ML*TS] packed (side << 16 | pixel)
-  int* nzlist = tlist + 2 * ML * TS;                     // [nb]
-  __shared__ int s_T0, s_T1, s_nnz, s_maxspan;
+  int* plist = span + 2 * ML;                            // [2*ML] packed (side << 16 | pixel)
+  __shared__ int s_T0, s_T1, s_maxspan, s_cnt;
+  __shared__ long long s_item;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double* colS = p.col + (size_t)blockIdx.x * 2 * 2 * ML * TS * np;   // [2 sides][ML][TS][np]
   double* colL = colS + (size_t)2 * ML * TS * np;
-  double* myS = wcol + (size_t)warp * 2 * TS * np;
+  double* myS = stage + (size_t)warp * 2 * TS * np;
   double* myL = myS + TS * np;
+  double* AS = stage;                  // [CH][NPAD] rows of bin t, scaled by k_S
+  double* AL = AS + CH * NPAD;         // [CH][NPAD] rows of bin t, scaled by k_L
+  double* BS = AL + CH * NPAD;         // [CH][NPAD] rows of bin u
+  double* BL = BS + CH * NPAD;
+  const int rgroups = (np + TR - 1) / TR, cgroups = (np + TC - 1) / TC, ntiles = rgroups * cgroups;
 
-  for (int64_t t = blockIdx.x; t < p.n_items; t += gridDim.x) {
-    const int a = p.f1[t], b = p.f2[t];
+  for (;;) {
+    if (tid == 0) s_item = (long long)atomicAdd(p.next, 1ull);
+    __syncthreads();
+    const long long t_item = s_item;
+    if (t_item >= p.n_items) break;
+    const int a = p.f1[t_item], b = p.f2[t_item];
     const int L1 = p.len[a], L2 = p.len[b];
-    if (L1 <= 0 || L2 <= 0) continue;
+    if (L1 <= 0 || L2 <= 0) { __syncthreads(); continue; }
     double c = lya_cos12(p.ux[a], p.uy[a], p.uz[a], p.ux[b], p.uy[b], p.uz[b], p.cos_variant);
     c = fmin(1.0, fmax(-1.0, c));
     const double ch = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(1.0, c)));
@@ -117,9 +138,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
     }
     if (tid == 0) { s_T0 = INT_MAX; s_T1 = -1; s_maxspan = 0; }
     __syncthreads();
-
-    // ---- columns, one warp per pixel: side 0 = f1 pixels (partners in f2),
-    // side 1 = f2 pixels (partners in f1); built in shared memory with the
+    // ---- phase 1: columns, one warp per pixel: side 0 = f1 pixels (partners in
+    // f2), side 1 = f2 pixels (partners in f1); built in shared memory with the
     // lanes over the partners, then stored to the CTA's scratch
     for (int side = 0; side < 2; ++side) {
       const int Lm = side == 0 ? L1 : L2, Lo = side == 0 ? L2 : L1;
@@ -193,95 +213,127 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
       __syncthreads();
       continue;
     }
-    const int nT = T1 - T0 + 1;
-    // ---- pixels per rt bin: tlist[tcount[t-T0] ..] = (side << 16 | pixel) whose span covers t
-    for (int k = tid; k <= nT; k += DT) tcount[k] = 0;
-    __syncthreads();
-    for (int side = 0; side < 2; ++side) {
-      const int Lm = side == 0 ? L1 : L2;
-      for (int m = tid; m < Lm; m += DT)
-        for (int s = 0; s < span[side * ML + m]; ++s) atomicAdd(&tcount[tlo[side * ML + m] + s - T0 + 1], 1);
+    for (int e = tid; e < 4 * nt * np; e += DT) {
+      const int tb = (e / np) % nt;
+      if (tb >= T0 && tb <= T1) mom[e] = 0.0;
     }
     __syncthreads();
-    if (tid == 0) {
-      for (int k = 1; k <= nT; ++k) tcount[k] += tcount[k - 1];
-      for (int k = 0; k < nT; ++k) tfill[k] = tcount[k];
-    }
-    __syncthreads();
-    for (int side = 0; side < 2; ++side) {
-      const int Lm = side == 0 ? L1 : L2;
-      for (int m = tid; m < Lm; m += DT)
-        for (int s = 0; s < span[side * ML + m]; ++s) {
-          const int pos = atomicAdd(&tfill[tlo[side * ML + m] + s - T0], 1);
-          tlist[pos] = (side << 16) | m;
-        }
-    }
-    __syncthreads();
-
-    // ---- moments of the touched bins (side 0 columns): entry e = (bp, t - T0)
-    const int ne = np * nT;
-    for (int e = tid; e < ne; e += DT) {
-      const int bp = e % np, tt = e / np, tb = T0 + tt;
-      double m0 = 0.0, mi = 0.0, mj = 0.0, mij = 0.0;
-      for (int q = tcount[tt]; q < tcount[tt + 1]; ++q) {
-        const int pk = tlist[q];
-        if ((pk >> 16) != 0) continue;
-        const int i = pk & 0xffff;
-        const size_t off = ((size_t)i * TS + (tb - tlo[i])) * np + bp;
-        const double s = colS[off], l = colL[off];
-        const double wi = sw[i], wli = sw[i] * sl[i];
-        m0 += wi * s; mj += wi * l; mi += wli * s; mij += wli * l;
-      }
-      mom[0 * nb + e] = m0; mom[1 * nb + e] = mi; mom[2 * nb + e] = mj; mom[3 * nb + e] = mij;
-    }
-    if (tid == 0) s_nnz = 0;
-    __syncthreads();
-    for (int e = tid; e < ne; e += DT) {
-      const double m0 = mom[e];
-      if (m0 != 0.0 || mom[nb + e] != 0.0 || mom[2 * nb + e] != 0.0 || mom[3 * nb + e] != 0.0) {
-        const int A = (e % np) * nt + T0 + e / np;
-        if (m0 != 0.0) {
-          atomicAdd(&p.W[A], m0);
-          atomicAdd(&p.D[(size_t)A * nb + A], m0);
-        }
-        nzlist[atomicAdd(&s_nnz, 1)] = e;
-      }
-    }
-    __syncthreads();
-    // ---- rank-4 part over touched bins
-    const int nnz = s_nnz;
     const double cA = 1.0 / (om1 * om2), cB = io2 / om1, cC = io1 / om2, cD = io1 * io2;
-    for (int64_t q = tid; q < (int64_t)nnz * nnz; q += DT) {
-      const int e1 = nzlist[q / nnz], e2 = nzlist[q % nnz];
-      const double v = mom[e1] * mom[e2] * cA + mom[2 * nb + e1] * mom[2 * nb + e2] * cB +
-                       mom[nb + e1] * mom[nb + e2] * cC + mom[3 * nb + e1] * mom[3 * nb + e2] * cD;
-      if (v != 0.0) {
-        const int A = (e1 % np) * nt + T0 + e1 / np;
-        const int B = (e2 % np) * nt + T0 + e2 / np;
-        atomicAdd(&p.D[(size_t)A * nb + B], v);
+    // ---- phase 2: blocks (t, u), T0 <= t <= u <= T1, diagonal blocks first
+    const int nT = T1 - T0 + 1;
+    const int nblk = nT + nT * (nT - 1) / 2;
+    for (int kb = 0; kb < nblk; ++kb) {
+      int t, u;
+      if (kb < nT) { t = u = T0 + kb; }
+      else {   // off-diagonal pairs in row-major order of the upper triangle
+        int r = kb - nT, tt = 0;
+        while (r >= nT - 1 - tt) { r -= nT - 1 - tt; ++tt; }
+        t = T0 + tt; u = t + 1 + r;
       }
-    }
-    // ---- column products: blocks (t, u) of rt bins, 50 x 50 (rp x rp) entries each
-    for (int tt = 0; tt < nT; ++tt) {
-      for (int uu = max(0, tt - (maxspan - 1)); uu <= min(nT - 1, tt + (maxspan - 1)); ++uu) {
-        const int tb = T0 + tt, ub = T0 + uu;
-        for (int e = tid; e < np * np; e += DT) {
-          const int bp = e / np, bq = e - bp * np;
-          double g = 0.0;
-          for (int q = tcount[tt]; q < tcount[tt + 1]; ++q) {
-            const int pk = tlist[q];
-            const int side = pk >> 16, m = pk & 0xffff;
+      double acc[TPT][TR * TC];
+#pragma unroll
+      for (int k = 0; k < TPT; ++k)
+#pragma unroll
+        for (int q = 0; q < TR * TC; ++q) acc[k][q] = 0.0;
+      if (u - t < maxspan) {
+        // pixels whose column spans both t and u
+        if (tid == 0) s_cnt = 0;
+        __syncthreads();
+        for (int side = 0; side < 2; ++side) {
+          const int Lm = side == 0 ? L1 : L2;
+          for (int m = tid; m < Lm; m += DT) {
             const int lo = tlo[side * ML + m], sp = span[side * ML + m];
-            if (ub < lo || ub >= lo + sp) continue;
-            const double* cS = colS + (size_t)side * ML * TS * np + (size_t)m * TS * np;
-            const double* cL = colL + (size_t)side * ML * TS * np + (size_t)m * TS * np;
-            const double wm = sw[side * ML + m];
-            const double kS = side == 0 ? wm / om2 : wm / om1;
-            const double kL = side == 0 ? wm * io2 : wm * io1;
-            g += kS * cS[(tb - lo) * np + bp] * cS[(ub - lo) * np + bq] +
-                 kL * cL[(tb - lo) * np + bp] * cL[(ub - lo) * np + bq];
+            if (sp > 0 && lo <= t && u < lo + sp) plist[atomicAdd(&s_cnt, 1)] = (side << 16) | m;
           }
-          if (g != 0.0) atomicAdd(&p.D[(size_t)(bp * nt + tb) * nb + (bq * nt + ub)], -g);
+        }
+        __syncthreads();
+        const int n = s_cnt;
+        for (int c0 = 0; c0 < n; c0 += CH) {
+          const int rows = min(CH, n - c0);
+          for (int e = tid; e < rows * NPAD; e += DT) {
+            const int r = e / NPAD, bq = e - r * NPAD;
+            const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
+            double vs = 0.0, vl = 0.0, us = 0.0, ul = 0.0;
+            if (bq < np) {
+              const int lo = tlo[side * ML + m];
+              const double* cs = colS + (size_t)side * ML * TS * np + (size_t)m * TS * np;
+              const double* cl = colL + (size_t)side * ML * TS * np + (size_t)m * TS * np;
+              const double wm = sw[side * ML + m];
+              const double kS = side == 0 ? wm / om2 : wm / om1;
+              const double kL = side == 0 ? wm * io2 : wm * io1;
+              vs = kS * cs[(t - lo) * np + bq];
+              vl = kL * cl[(t - lo) * np + bq];
+              us = cs[(u - lo) * np + bq];
+              ul = cl[(u - lo) * np + bq];
+            }
+            AS[r * NPAD + bq] = vs; AL[r * NPAD + bq] = vl; BS[r * NPAD + bq] = us; BL[r * NPAD + bq] = ul;
+          }
+          __syncthreads();
+          if (t == u) {   // moments of bin t from the unscaled rows of the f1 pixels
+            for (int e = tid; e < 4 * np; e += DT) {
+              const int q = e / np, bq = e - q * np;
+              const double* src = q < 2 ? BS : BL;   // 0: M0, 1: Mi from S; 2: Mj, 3: Mij from L
+              double sacc = 0.0;
+              for (int r = 0; r < rows; ++r) {
+                const int pk = plist[c0 + r];
+                if ((pk >> 16) != 0) continue;
+                const int m = pk & 0xffff;
+                const double cw = (q == 0 || q == 2) ? sw[m] : sw[m] * sl[m];
+                sacc += cw * src[r * NPAD + bq];
+              }
+              mom[(q * nt + t) * np + bq] += sacc;
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            const int tile = tid + k * DT;
+            if (tile < ntiles) {
+              const int r0 = (tile / cgroups) * TR, q0 = (tile % cgroups) * TC;
+              for (int r = 0; r < rows; ++r) {
+                const double* as = AS + r * NPAD + r0;
+                const double* bs = BS + r * NPAD + q0;
+                const double* al = AL + r * NPAD + r0;
+                const double* bl = BL + r * NPAD + q0;
+#pragma unroll
+                for (int i = 0; i < TR; ++i)
+#pragma unroll
+                  for (int j = 0; j < TC; ++j) acc[k][i * TC + j] = fma(as[i], bs[j], fma(al[i], bl[j], acc[k][i * TC + j]));
+              }
+            }
+          }
+          __syncthreads();
+        }
+      }
+      // flush: column products (subtracted), rank-4 part, diagonal
+#pragma unroll
+      for (int k = 0; k < TPT; ++k) {
+        const int tile = tid + k * DT;
+        if (tile < ntiles) {
+          const int r0 = (tile / cgroups) * TR, q0 = (tile % cgroups) * TC;
+#pragma unroll
+          for (int i = 0; i < TR; ++i) {
+            const int bp = r0 + i;
+            if (bp >= np) continue;
+            const double* mt = mom + (size_t)t * np + bp;   // + q*nt*np
+            const double m0a = mt[0], mia = mt[nt * np], mja = mt[2 * nt * np], mija = mt[3 * nt * np];
+#pragma unroll
+            for (int j = 0; j < TC; ++j) {
+              const int bq = q0 + j;
+              if (bq >= np) continue;
+              const double* mu = mom + (size_t)u * np + bq;
+              double v = m0a * mu[0] * cA + mja * mu[2 * nt * np] * cB + mia * mu[nt * np] * cC +
+                         mija * mu[3 * nt * np] * cD - acc[k][i * TC + j];
+              const int A = bp * nt + t, B = bq * nt + u;
+              if (A == B) {
+                v += m0a;
+                if (m0a != 0.0) atomicAdd(&p.W[A], m0a);
+              }
+              if (v != 0.0) {
+                atomicAdd(&p.D[(size_t)A * nb + B], v);
+                if (t != u) atomicAdd(&p.D[(size_t)B * nb + A], v);
+              }
+            }
+          }
         }
       }
     }
@@ -297,14 +349,17 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   if (ctx->cat.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_dist_run: no forests uploaded");
   if (!ctx->cat.has_dl || !ctx->cat.has_moments)
     return lya_fail(ctx, LYA_ERR_STATE, "lya_dist_run: upload dl, omega and odl2 with the forests");
-  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
   const int np = ctx->np, nt = ctx->nt, nb = np * nt;
+  if (np > NP_MAX) return lya_fail(ctx, LYA_ERR_ARG, "lya_dist_run: np = %d above %d r_par bins", np, NP_MAX);
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
   int max_len = 1;
   for (int64_t f = 0; f < ctx->cat.n; ++f)
     max_len = std::max<int>(max_len, (int)(ctx->h_start[f + 1] - ctx->h_start[f]));
   if (max_len > 65535) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests longer than 65535 pixels");
-  const size_t smem = sizeof(double) * (6 * (size_t)max_len + 4 * (size_t)nb + (size_t)NW * 2 * TS * np) +
-                      sizeof(int) * (4 * (size_t)max_len + 2 * (nt + 1) + 2 * (size_t)max_len * TS + nb);
+  const int npad = std::max(TR * ((np + TR - 1) / TR), TC * ((np + TC - 1) / TC));
+  const size_t stage_len = std::max<size_t>((size_t)4 * CH * npad, (size_t)NW * 2 * TS * np);
+  const size_t smem = sizeof(double) * (6 * (size_t)max_len + 4 * (size_t)nt * np + stage_len) +
+                      sizeof(int) * (6 * (size_t)max_len);
   if (smem > 227 * 1024)
     return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory", max_len, smem);
   const int grid = ctx->num_sms;
@@ -313,7 +368,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   cudaError_t e = lya_alloc(&d_D, (size_t)nb * nb);
   if (e == cudaSuccess) e = lya_alloc(&d_W, nb);
   if (e == cudaSuccess) e = lya_alloc(&col, (size_t)grid * 2 * 2 * max_len * TS * np);
-  if (e == cudaSuccess) e = lya_alloc(&err, 1);
+  if (e == cudaSuccess) e = lya_alloc(&err, 2);
   auto cleanup = [&]() { lya_free(d_D); lya_free(d_W); lya_free(col); lya_free(err); };
   if (e != cudaSuccess) {
     cleanup();
@@ -322,7 +377,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   cudaStream_t s = ctx->stream;
   e = cudaMemsetAsync(d_D, 0, sizeof(double) * (size_t)nb * nb, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_W, 0, sizeof(double) * nb, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 2 * sizeof(unsigned long long), s);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
   if (e == cudaSuccess && ctx->wq.n_pairs > 0) {
     DistParams p;
@@ -331,8 +386,8 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     p.omega = ctx->cat.omega; p.odl2 = ctx->cat.odl2; p.f1 = ctx->wq.f1; p.f2 = ctx->wq.f2;
     p.n_items = ctx->wq.n_pairs; p.max_len = max_len;
     p.binner_rp = (double)np / ctx->rpmax; p.binner_rt = (double)nt / ctx->rtmax;
-    p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant;
-    p.col = col; p.D = d_D; p.W = d_W; p.err = err;
+    p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant; p.npad = npad;
+    p.col = col; p.D = d_D; p.W = d_W; p.err = err; p.next = err + 1;
     e = cudaFuncSetAttribute(k_dist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) {
       k_dist<<<grid, DT, smem, s>>>(p);

@@ -18,6 +18,13 @@
 // of a forest without bounds checks (the values are never used).
 #define LYA_MARGIN 64
 
+// Per-forest flags (DevCatalog::sorted): dc non-decreasing; and, in addition,
+// every dc finite and in [0, LYA_LEAN_DC_MAX), which the lean walk of the FP32
+// kernel requires for its error bound.
+#define LYA_SORTED 1
+#define LYA_LEAN 2
+#define LYA_LEAN_DC_MAX 1.0e6
+
 // Device-side statistics slots (unsigned long long counters).
 enum { ST_EVALUATED = 0, ST_RECHECK = 1, ST_RUNS = 2, ST_INRANGE = 3, ST_ERROR = 4, ST_N = 8 };
 
@@ -32,7 +39,7 @@ struct DevCatalog {
   int32_t n_slots = 0;
   int64_t* pstart = nullptr;   // [n]
   int32_t* len = nullptr;      // [n]
-  uint8_t* sorted = nullptr;   // [n] 1 when dc is non-decreasing
+  uint8_t* sorted = nullptr;   // [n] LYA_SORTED | LYA_LEAN flags
   int32_t* slot = nullptr;     // [n] owner histogram
   double* ux = nullptr;        // [n]
   double* uy = nullptr;

@@ -16,6 +16,12 @@ pytestmark = pytest.mark.gpu
 
 KERNELS = [N.KERNEL_FP32_GUARDED, N.KERNEL_FP64_DIAGONAL, N.KERNEL_FP64_PLAIN]
 TOL = {N.KERNEL_FP32_GUARDED: 1e-6, N.KERNEL_FP64_DIAGONAL: 1e-12, N.KERNEL_FP64_PLAIN: 1e-12}
+# (kernel, walk variant): the FP32 kernel with its default walk (lean walk for
+# eligible forest pairs) and with the two-diagonal walk for every pair, and the
+# two FP64 kernels
+CASES = [(N.KERNEL_FP32_GUARDED, 0), (N.KERNEL_FP32_GUARDED, N.VARIANT_TWO_DIAGONALS), (N.KERNEL_FP64_DIAGONAL, 0),
+         (N.KERNEL_FP64_PLAIN, 0)]
+CASE_IDS = ['fp32', 'fp32-diag2', 'fp64diag', 'fp64plain']
 
 
 def check_hist(h, c, ho, co, kern, label=''):
@@ -52,12 +58,12 @@ def test_device_neighbours_equal_oracle(cfg0):
     assert st['ref_pairs'] == float(np.sum(fs.lengths[o1] * fs.lengths[nbr]))
 
 
-@pytest.mark.parametrize('kern', KERNELS)
-def test_config0_slots_match_oracle(cfg0, kern):
+@pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
+def test_config0_slots_match_oracle(cfg0, kern, var):
     fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
     ns = 4
     ho, co = O.corr(fs, f1[:sis[ns]], f2[:sis[ns]], sis[:ns + 1])
-    eng.run(kernel=kern)
+    eng.run(kernel=kern, variant=var)
     h, c = eng.histograms(0, ns)
     check_hist(h, c, ho, co, kern, f'kernel {kern}')
 
@@ -72,18 +78,20 @@ def test_slot_restricted_run(cfg0):
     assert st['run_ref_pairs'] == float(np.sum(fs.lengths[f1[sis[3]:sis[5]]] * fs.lengths[f2[sis[3]:sis[5]]]))
 
 
-def test_fp32_counts_equal_fp64_all_slots(cfg0):
+@pytest.mark.parametrize('var', [0, N.VARIANT_TWO_DIAGONALS], ids=['fp32', 'fp32-diag2'])
+def test_fp32_counts_equal_fp64_all_slots(cfg0, var):
     fs, am, eng, _, _ = cfg0
-    eng.run(kernel=N.KERNEL_FP32_GUARDED)
+    eng.run(kernel=N.KERNEL_FP32_GUARDED, variant=var)
     h32, c32 = eng.histograms()
     eng.run(kernel=N.KERNEL_FP64_DIAGONAL)
     h64, c64 = eng.histograms()
     assert np.array_equal(c32, c64)
-    np.testing.assert_allclose(h32[:, N.Q_W], h64[:, N.Q_W], rtol=1e-6, atol=0)
+    for q in (N.Q_W, N.Q_RP, N.Q_RT, N.Q_Z):
+        np.testing.assert_allclose(h32[:, q], h64[:, q], rtol=1e-6, atol=0)
 
 
-@pytest.mark.parametrize('kern', KERNELS)
-def test_edge_catalog(kern):
+@pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
+def test_edge_catalog(kern, var):
     fs = E.edge_catalog()
     am = 0.05
     with PairEngine() as eng:
@@ -94,21 +102,21 @@ def test_edge_catalog(kern):
         d1, d2 = eng.get_pairs()
         assert set(zip(d1.tolist(), d2.tolist())) == set(zip(f1.tolist(), f2.tolist()))
         ho, co = O.corr(fs, f1, f2, sis)
-        eng.run(kernel=kern)
+        eng.run(kernel=kern, variant=var)
         h, c = eng.histograms()
         check_hist(h, c, ho, co, kern, 'edge catalogue')
         assert c.sum() > 0
 
 
-@pytest.mark.parametrize('kern', KERNELS)
-def test_adversarial_bin_edges_bit_exact(kern):
+@pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
+def test_adversarial_bin_edges_bit_exact(kern, var):
     """Pairs within a few ulps of an rt edge: the FP32 kernel must fall back to
     the FP64 formula and land where the oracle does."""
     fs, f1, f2, vb = E.cos_variant_cases(192)
     with PairEngine() as eng:
         eng.upload(fs)
         eng.set_pairs(f1, f2)
-        st = eng.run(kernel=kern)
+        st = eng.run(kernel=kern, variant=var)
         h, c = eng.histograms()
     got = np.array([int(np.nonzero(c[s])[0][0]) if c[s].sum() else -1 for s in range(len(f1))])
     assert np.array_equal(got, vb[:, 0])
@@ -153,7 +161,36 @@ def test_unsorted_and_empty_forests_full_walk():
         off, nbr = O.neighbours(fs, am)
         f1, f2, sis, _ = O.items_from_csr(fs, off, nbr)
         ho, co = O.corr(fs, f1, f2, sis)
-        for kern in KERNELS:
-            eng.run(kernel=kern)
+        for kern, var in CASES:
+            eng.run(kernel=kern, variant=var)
             h, c = eng.histograms()
-            check_hist(h, c, ho, co, kern, f'unsorted {kern}')
+            check_hist(h, c, ho, co, kern, f'unsorted {kern}/{var}')
+
+
+def test_lean_walk_mixed_with_ineligible_forests():
+    """The FP32 kernel's lean walk takes pairs of sorted forests with
+    0 <= dc < 1e6 only; forests with negative or very large dc, or a NaN pixel,
+    fall back to the two-diagonal walk in the same launch.  Counts and sums
+    match the oracle."""
+    fs = synthetic.make(4, n=60)
+    am = synthetic.angmax_for(fs)
+    for f in range(0, fs.n, 5):          # shifted below zero (still sorted)
+        a, b = fs.start[f], fs.start[f + 1]
+        fs.dc[a:b] -= fs.dc[a] + 50.0
+    for f in range(1, fs.n, 7):          # beyond the lean range
+        a, b = fs.start[f], fs.start[f + 1]
+        fs.dc[a:b] += 2.0e6
+    for f in range(2, fs.n, 11):         # one NaN pixel
+        a, b = fs.start[f], fs.start[f + 1]
+        if b - a > 3:
+            fs.dc[a + 2] = np.nan
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.build_pairs(am)
+        off, nbr = O.neighbours(fs, am)
+        f1, f2, sis, _ = O.items_from_csr(fs, off, nbr)
+        ho, co = O.corr(fs, f1, f2, sis)
+        eng.run(kernel=N.KERNEL_FP32_GUARDED)
+        h, c = eng.histograms()
+    check_hist(h, c, ho, co, N.KERNEL_FP32_GUARDED, 'lean walk with ineligible forests')
+    assert c.sum() > 0
