@@ -52,6 +52,10 @@ def parse():
     ap.add_argument('--cpu-seconds', type=float, default=15.0, help='target CPU-baseline sample duration')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-compare', action='store_true', help='skip the FP64 comparison sample')
+    ap.add_argument('--no-autotune', action='store_true', help='library default walk instead of the autotuned one')
+    ap.add_argument('--dist-scale', type=float, default=0.03,
+                    help='distortion sample: fraction of the 30,000-forest distortion catalogue (0 = skip)')
+    ap.add_argument('--no-adjoint', action='store_true', help='skip the adjoint timing')
     return ap.parse_args()
 
 
@@ -155,45 +159,37 @@ class ClockSampler:
 # ---------------------------------------------------------------- CPU baseline (oracle port)
 def cpu_baseline(fs, angmax, seconds, seed=5):
     """Time the CPU restatement of the reference kernel (oracle) on a bounded,
-    seeded sample of owner pixels of the same catalogue, all host cores."""
+    seeded sample of the same catalogue's work, all host cores: forest pairs
+    (the reference's per-launch unit) in a seeded random order, in batches of
+    one chunk of about 1e8 pixel pairs per core, until the elapsed time
+    reaches ``seconds``."""
     from oracle import oracle as O
     cores = len(os.sched_getaffinity(0))
     off, nbr = O.neighbours(fs, angmax, nthreads=cores)
     f1, f2, sis, pixels = O.items_from_csr(fs, off, nbr)
-    L = fs.lengths
-    slot_pairs = np.array([np.sum(L[f1[sis[s]:sis[s + 1]]] * L[f2[sis[s]:sis[s + 1]]]) for s in range(len(pixels))],
-                          dtype=np.float64)
-    rng = np.random.default_rng(seed)
-    order = rng.permutation(len(pixels))
-    # calibrate the single-core rate on ~3e8 pixel pairs of one pixel, then take
-    # enough pixels for the target duration on all cores
-    s0 = order[0]
-    it = np.arange(sis[s0], sis[s0 + 1])
-    csum = np.cumsum(L[f1[it]] * L[f2[it]])
-    m = min(int(np.searchsorted(csum, 3e8)) + 1, len(it))
-    t = time.perf_counter()
-    O.corr(fs, f1[it[:m]], f2[it[:m]], np.array([0, m]), nthreads=1)
-    dt = max(time.perf_counter() - t, 1e-3)
-    rate1 = max(float(csum[min(m, len(csum)) - 1]) / dt, 1e7)
-    target = rate1 * cores * seconds
-    chosen, acc = [], 0.0
-    for s in order:
-        chosen.append(s)
-        acc += slot_pairs[s]
-        if acc >= target or len(chosen) >= 4 * cores and acc >= 0.5 * target:
-            break
-    chosen = np.array(sorted(chosen))
-    idx = np.concatenate([np.arange(sis[s], sis[s + 1]) for s in chosen])
-    cnts = np.array([sis[s + 1] - sis[s] for s in chosen])
-    sis_c = np.zeros(len(chosen) + 1, dtype=np.int64)
-    np.cumsum(cnts, out=sis_c[1:])
-    t = time.perf_counter()
-    O.corr(fs, f1[idx], f2[idx], sis_c, nthreads=cores)
-    dt = time.perf_counter() - t
-    pairs = float(np.sum(slot_pairs[chosen]))
+    L = fs.lengths.astype(np.float64)
+    order = np.random.default_rng(seed).permutation(len(f1))
+    cost = L[f1[order]] * L[f2[order]]
+    csum = np.cumsum(cost)
+    done, pairs, dt, calls = 0, 0.0, 0.0, 0
+    while done < len(order) and dt < seconds:
+        # the next `cores` chunks of ~1e8 pixel pairs each, one per thread
+        base = csum[done - 1] if done else 0.0
+        bounds = np.searchsorted(csum, base + 1e8 * np.arange(1, cores + 1), side='right')
+        bounds = np.minimum(np.maximum(bounds, done + 1), len(order))
+        cuts = np.unique(np.concatenate([[done], bounds]))
+        idx = order[cuts[0]:cuts[-1]]
+        sis_c = (cuts - cuts[0]).astype(np.int64)
+        t = time.perf_counter()
+        O.corr(fs, f1[idx], f2[idx], sis_c, nthreads=cores)
+        dt += time.perf_counter() - t
+        pairs += float(np.sum(cost[cuts[0]:cuts[-1]]))
+        done = int(cuts[-1])
+        calls += 1
     return {'value': pairs / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-            'sample': f'{len(chosen)} of {len(pixels)} owner pixels (seeded), {pairs:.3e} pixel pairs, '
-                      f'{dt:.1f} s; FP64 every pixel pair like the reference kernel',
+            'sample': f'{done} of {len(f1)} forest pairs (seeded random order, {calls} calls of {cores} chunks of '
+                      f'~1e8 pixel pairs), {pairs:.3e} pixel pairs, {dt:.1f} s; FP64 every pixel pair like the '
+                      f'reference kernel',
             'seconds': dt, 'pairs': pairs}
 
 
@@ -255,19 +251,23 @@ def run_b200(args, dist):
         eng.build_pairs(angmax)
         return eng.run(kernel=kern, guard=GUARD)
 
-    for _ in range(args.warmup):
+    tune = None
+    for k in range(args.warmup):
+        if k == 1 and not args.no_autotune:   # after the first warm-up step: choose the walk, then warm it
+            tune = eng.autotune(kernel=kern, guard=GUARD)
         step()
     st0 = eng.stats()
     launches0 = st0['launches']
     dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(dev) if dist.rank == 0 else None
-    kernel_ms, build_ms = [], []
+    kernel_ms, build_ms, run_ms = [], [], []
     eng.timer_start()
     for _ in range(args.steps):
         st = step()
         kernel_ms.append(st['kernel_ms'])
         build_ms.append(st['build_ms'])
+        run_ms.append(st['run_ms'])
     dev_ms = eng.timer_stop()
     torch.cuda.synchronize()
     dist.barrier()
@@ -318,6 +318,22 @@ def run_b200(args, dist):
         e2e_s = dist.max(time.perf_counter() - t)
         e2e_value = dist.sum(ref_pairs * args.e2e_steps) / e2e_s
 
+    # ---- adjoint (gradient of sum_b g_b DW_b/W_b w.r.t. dw and w of every pixel) on the same catalogue
+    adjoint = None
+    if not args.no_adjoint:
+        g = np.random.default_rng(4).normal(size=eng.nb)
+        gdw = torch.empty(fs.npix_total, dtype=torch.float64, device=f'cuda:{dev}')
+        gw = torch.empty_like(gdw)
+        eng.adjoint(g, out_dw=gdw, out_w=gw)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        eng.adjoint(g, out_dw=gdw, out_w=gw)
+        torch.cuda.synchronize()
+        adj_s = time.perf_counter() - t
+        adjoint = {'seconds': adj_s, 'ref_pixel_pairs_per_s': ref_pairs / adj_s,
+                   'what': 'one lya_corr_adjoint call (device gradients) over the whole work queue, wall clock',
+                   'forward_kernel_ms': float(np.median(kernel_ms))}
+
     out = None
     if dist.rank == 0:
         # ---- FP32 vs FP64 on a sample of owner slots: bit-exact counts and pairs/s
@@ -338,6 +354,7 @@ def run_b200(args, dist):
                 'note': 'not HBM-bound: the forests are re-read from L2; the bound is FP32 issue (see alu)',
                 'alu': alu_roofline(st, kms, clk)}
         cpu = None if args.no_cpu_baseline else cpu_baseline(fs, angmax, args.cpu_seconds)
+        distortion = None if args.dist_scale <= 0 else distortion_sample(args.dist_scale, dev)
         ms_step = t_max / args.steps
         out = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': dist.world, 'steps': args.steps,
                'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
@@ -351,6 +368,8 @@ def run_b200(args, dist):
                           'parallelism': f'weak: {dist.world} rank(s), one catalogue each'},
                'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                        'path': 'lya_upload_forests + lya_build_pairs + lya_corr_run + lya_corr_get, pinned host'},
+               'tuned': tune, 'kernel_ms_steps': kernel_ms, 'run_ms_steps': run_ms, 'build_ms_steps': build_ms,
+               'distortion': distortion, 'adjoint': adjoint,
                'gpu_launches': int(launches),
                'kernel_ms': kms, 'build_ms': float(np.median(build_ms)),
                'evaluated_pairs_per_step': st['evaluated_pairs'], 'guard_rechecks_per_step': st['guard_rechecks'],
@@ -358,6 +377,28 @@ def run_b200(args, dist):
                'roofline': roof, 'clocks': clk, 'cpu_baseline': cpu, 'fp64_comparison': compare}
     eng.close()
     return out
+
+
+def distortion_sample(scale, dev):
+    """Distortion matrix (all neighbouring forest pairs, no subsampling) of a
+    seeded sample of the 30,000-forest log-normal distortion catalogue:
+    ``scale`` of its forests on the same sky density."""
+    from lya2pcf_b200 import synthetic
+    from lya2pcf_b200.engine import PairEngine
+    fs = synthetic.make(3, scale=scale)
+    am = synthetic.angmax_for(fs)
+    with PairEngine(device=dev) as eng:
+        eng.upload(fs)
+        n = eng.build_pairs(am)
+        f1, f2 = eng.get_pairs()
+        L = fs.lengths.astype(np.float64)
+        ref = float(np.sum(L[f1] * L[f2]))
+        eng.distortion()
+        D, W = eng.distortion()
+        ms = eng.stats()['kernel_ms']
+    return {'forests': fs.n, 'scale': scale, 'forest_pairs': n, 'ref_pixel_pairs': ref, 'kernel_ms': ms,
+            'forest_pairs_per_s': n / (ms * 1e-3), 'ref_pixel_pairs_per_s': ref / (ms * 1e-3),
+            'matrix': f'{D.shape[0]}x{D.shape[1]} float64, {int(np.count_nonzero(D))} nonzero'}
 
 
 def fp64_comparison(eng, fs, kern):

@@ -53,6 +53,9 @@ typedef struct {
                               0 <= dc < 1e6, walk 2 for the others; FP64: one
                               diagonal per lane), 1 = one diagonal per lane,
                               2 = two diagonals per lane, 3 = same as 0 */
+  int32_t run_cap;         /* longest register run of the diagonal walks before it
+                              is recorded (bounds FP32 run sums): 0 = default
+                              (128), else a power of two in [8, 1024] */
 } lya_corr_opts;
 
 typedef struct {

@@ -56,7 +56,7 @@ class LyaError(RuntimeError):
 class CorrOpts(C.Structure):
     _fields_ = [('kernel', C.c_int32), ('guard', C.c_double), ('warps_per_block', C.c_int32),
                 ('blocks_per_sm', C.c_int32), ('slot_begin', C.c_int32), ('slot_end', C.c_int32),
-                ('variant', C.c_int32)]
+                ('variant', C.c_int32), ('run_cap', C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -41,6 +41,16 @@ void lya_free_queue(WorkQueue& q) {
   q = WorkQueue{};
 }
 
+cudaError_t lya_queue_reserve(WorkQueue& q, int64_t n) {
+  if (n <= q.cap && q.f1 && q.f2) return cudaSuccess;
+  lya_free_queue(q);
+  cudaError_t e = lya_alloc(&q.f1, (size_t)std::max<int64_t>(n, 1));
+  if (e == cudaSuccess) e = lya_alloc(&q.f2, (size_t)std::max<int64_t>(n, 1));
+  if (e != cudaSuccess) { lya_free_queue(q); return e; }
+  q.cap = std::max<int64_t>(n, 1);
+  return cudaSuccess;
+}
+
 extern "C" int lya_version(void) { return 10000; }
 
 extern "C" const char* lya_last_error(const lya_ctx* ctx) {
@@ -74,6 +84,9 @@ extern "C" int lya_ctx_create(int device, lya_ctx** out) {
     if ((e = cudaEventCreate(&ctx->tev0)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
     if ((e = cudaEventCreate(&ctx->tev1)) != cudaSuccess) { rc = LYA_ERR_CUDA; break; }
     if ((e = lya_alloc(&ctx->stats, ST_N)) != cudaSuccess) { rc = LYA_ERR_ALLOC; break; }
+    if ((e = cudaMallocHost((void**)&ctx->h_stats, sizeof(unsigned long long) * (ST_N + 1))) != cudaSuccess) {
+      rc = LYA_ERR_ALLOC; break;
+    }
   } while (0);
   if (rc != LYA_OK) {
     lya_fail(nullptr, rc, "lya_ctx_create: %s", cudaGetErrorString(e));
@@ -91,6 +104,10 @@ extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
   lya_free_catalog(ctx->cat);
   lya_free_queue(ctx->wq);
   lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
+  lya_free(ctx->cost);
+  if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
+  if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+  if (ctx->run_graph) cudaGraphExecDestroy(ctx->run_graph);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->ev2) cudaEventDestroy(ctx->ev2);
@@ -322,11 +339,10 @@ extern "C" int lya_set_pairs(lya_ctx* ctx, int64_t n_pairs, const int32_t* f1, c
   if (n_pairs < 0 || (n_pairs > 0 && (!f1 || !f2))) return lya_fail(ctx, LYA_ERR_ARG, "lya_set_pairs: bad arguments");
   if (ctx->cat.n == 0 && n_pairs > 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_set_pairs: upload forests first");
   LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
-  lya_free_queue(ctx->wq);
   ctx->have_result = false;
   WorkQueue& q = ctx->wq;
-  cudaError_t e = lya_alloc(&q.f1, n_pairs);
-  if (e == cudaSuccess) e = lya_alloc(&q.f2, n_pairs);
+  q.n_pairs = 0;
+  cudaError_t e = lya_queue_reserve(q, n_pairs);
   if (e != cudaSuccess) {
     lya_free_queue(q);
     return lya_fail(ctx, LYA_ERR_ALLOC, "lya_set_pairs: device allocation failed");

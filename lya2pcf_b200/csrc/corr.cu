@@ -29,6 +29,7 @@
 //   otherwise the pair is re-evaluated with the reference's FP64 formula.  The
 //   guard is checked on the host against a proven bound on the FP32 error, so
 //   every bin index (and hence every pair count) equals the FP64 formula's.
+#include <cub/device/device_scan.cuh>
 #include <thrust/binary_search.h>
 #include <thrust/execution_policy.h>
 #include <thrust/iterator/counting_iterator.h>
@@ -36,6 +37,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "lya_internal.cuh"
 
@@ -1152,13 +1154,21 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
 }
 
 template <int KIND, int WARPS>
+size_t corr_smem_bytes(const CorrParams& p, int nb) {
+  return (size_t)nb * (LYA_NQ * sizeof(double) + sizeof(unsigned long long)) +
+         (size_t)WARPS * REC * rec_bytes<KIND>() +
+         (KIND == LYA_KERNEL_FP32_GUARDED ? (size_t)WARPS * lean_ctl_stride(p.np, p.nt) * sizeof(float) : 0);
+}
+
+template <int KIND, int WARPS>
+cudaError_t set_corr_smem(const CorrParams& p, int nb) {
+  return cudaFuncSetAttribute(k_corr<KIND, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)corr_smem_bytes<KIND, WARPS>(p, nb));
+}
+
+template <int KIND, int WARPS>
 cudaError_t launch_corr(const CorrParams& p, int nctas, int nb, cudaStream_t s) {
-  const size_t smem = (size_t)nb * (LYA_NQ * sizeof(double) + sizeof(unsigned long long)) +
-                      (size_t)WARPS * REC * rec_bytes<KIND>() +
-                      (KIND == LYA_KERNEL_FP32_GUARDED ? (size_t)WARPS * lean_ctl_stride(p.np, p.nt) * sizeof(float) : 0);
-  cudaError_t e = cudaFuncSetAttribute(k_corr<KIND, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k_corr<KIND, WARPS><<<nctas, WARPS * 32, smem, s>>>(p);
+  k_corr<KIND, WARPS><<<nctas, WARPS * 32, corr_smem_bytes<KIND, WARPS>(p, nb), s>>>(p);
   return cudaGetLastError();
 }
 
@@ -1205,27 +1215,6 @@ __global__ void k_cta_bounds(int nctas, int64_t n, const long long* __restrict__
 
 }  // namespace
 
-int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out, int slot_begin, int slot_end,
-                           double* d_range_pairs) {
-  const int64_t n = ctx->wq.n_pairs;
-  long long* cost = nullptr;
-  cudaError_t e = lya_alloc(&cost, (size_t)std::max<int64_t>(n, 1));
-  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "cta ranges: allocation failed");
-  if (n > 0) {
-    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 16);
-    k_item_cost<<<blocks, 256, 0, ctx->stream>>>(n, ctx->wq.f1, ctx->wq.f2, ctx->cat.len, cost);
-    ctx->launches++;
-    thrust::inclusive_scan(thrust::cuda::par.on(ctx->stream), cost, cost + n, cost);
-  }
-  k_cta_bounds<<<(nctas + 1 + 127) / 128, 128, 0, ctx->stream>>>(nctas, n, cost, ctx->wq.f1, ctx->cat.slot, slot_begin,
-                                                                 slot_end, d_out, d_range_pairs);
-  ctx->launches++;
-  e = cudaGetLastError();
-  lya_free(cost);   // cudaFree waits for the queued work
-  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "cta ranges: %s", cudaGetErrorString(e));
-  return LYA_OK;
-}
-
 // Largest FP32 error of a bin coordinate (bin units) for coordinates below
 // `reach` bins: four roundings of relative size 2^-24 (hi-difference and lo sum,
 // the FP32 factor ch*binner, the product) bound |x - x64| by 2^-22 x; the
@@ -1235,6 +1224,60 @@ static double guard_bound_bins(double reach) {
   const double rel = std::ldexp(1.0, -22) + std::ldexp(1.0, -50);
   const double ulp_reach = std::ldexp(1.0, (int)std::floor(std::log2(std::max(reach, 1.0))) - 23);
   return 1.1 * rel * reach + ulp_reach + 1e-12;
+}
+
+// Everything a captured run depends on: the kernel parameters and the
+// scratch and output buffers.  A run whose key differs from the captured one
+// is captured again.
+struct RunGraphKey {
+  CorrParams p;
+  int kind, nctas, nslots, nb;
+  int slot_begin, slot_end;
+  int64_t n_items;
+  const void* cost;
+  const void* scan_tmp;
+  size_t scan_bytes;
+};
+
+// The stream work of one run: clear the outputs, balance the work queue over
+// the CTAs (cost prefix sum), the persistent pair kernel, and the copy of the
+// counters to pinned host memory.  No allocation and no synchronisation, so it
+// is captured once in a CUDA graph and replayed.
+static cudaError_t enqueue_run(lya_ctx* ctx, const RunGraphKey& k, double* d_range_pairs, int slot_begin,
+                               int slot_end) {
+  cudaStream_t s = ctx->stream;
+  const CorrParams& p = k.p;
+  cudaError_t e = cudaEventRecordWithFlags(ctx->ev2, s, cudaEventRecordExternal);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(p.hist, 0, sizeof(double) * (size_t)k.nslots * LYA_NQ * 2 * k.nb, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p.counts, 0, sizeof(unsigned long long) * (size_t)k.nslots * k.nb, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p.stats, 0, sizeof(unsigned long long) * ST_N, s);
+  if (e == cudaSuccess && k.n_items > 0) {
+    const int blocks = (int)std::min<int64_t>((k.n_items + 255) / 256, (int64_t)ctx->num_sms * 16);
+    k_item_cost<<<blocks, 256, 0, s>>>(k.n_items, p.f1, p.f2, p.len, ctx->cost);
+    e = cudaGetLastError();
+    size_t bytes = k.scan_bytes;
+    if (e == cudaSuccess)
+      e = cub::DeviceScan::InclusiveSum(ctx->scan_tmp, bytes, ctx->cost, ctx->cost, k.n_items, s);
+  }
+  if (e == cudaSuccess) {
+    k_cta_bounds<<<(k.nctas + 1 + 127) / 128, 128, 0, s>>>(k.nctas, k.n_items, ctx->cost, p.f1, p.slot, slot_begin,
+                                                             slot_end, ctx->cta_begin, d_range_pairs);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev0, s, cudaEventRecordExternal);
+  if (e == cudaSuccess) {
+    if (k.kind == LYA_KERNEL_FP32_GUARDED) e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16>(p, k.nctas, k.nb, s);
+    else if (k.kind == LYA_KERNEL_FP64_DIAGONAL) e = launch_corr<LYA_KERNEL_FP64_DIAGONAL, 16>(p, k.nctas, k.nb, s);
+    else e = launch_corr<LYA_KERNEL_FP64_PLAIN, 16>(p, k.nctas, k.nb, s);
+  }
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev1, s, cudaEventRecordExternal);
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev3, s, cudaEventRecordExternal);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->h_stats, p.stats, sizeof(unsigned long long) * ST_N, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->h_stats + ST_N, d_range_pairs, sizeof(double), cudaMemcpyDeviceToHost, s);
+  return e;
 }
 
 int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
@@ -1253,7 +1296,7 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
                     "guard %.3g Mpc/h outside [%.3g, %.3g]: below the proven FP32 error bound or above a quarter bin",
                     o->guard, ctx->last.guard_bound, 0.25 * std::min(ctx->rpmax / ctx->np, ctx->rtmax / ctx->nt));
 
-  // outputs
+  // outputs and scratch (allocated once, reused by later runs)
   if (ctx->hist_slots != nslots || ctx->hist_nb != nb || !ctx->hist) {
     lya_free(ctx->hist); lya_free(ctx->counts);
     cudaError_t e = lya_alloc(&ctx->hist, (size_t)nslots * LYA_NQ * 2 * nb);
@@ -1265,12 +1308,6 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
     }
     ctx->hist_slots = nslots; ctx->hist_nb = nb;
   }
-  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev2, s));
-  LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->hist, 0, sizeof(double) * (size_t)nslots * LYA_NQ * 2 * nb, s));
-  LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->counts, 0, sizeof(unsigned long long) * (size_t)nslots * nb, s));
-  LYA_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->stats, 0, sizeof(unsigned long long) * ST_N, s));
-
-  const int warps = 16;
   const int nctas = ctx->num_sms * std::max(1, o->blocks_per_sm);
   if (ctx->cta_cap < nctas + 2) {
     lya_free(ctx->cta_begin);
@@ -1278,12 +1315,32 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
       return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_run: allocation failed");
     ctx->cta_cap = nctas + 2;
   }
-  // the slot of the range's reference pair count shares the cta_begin buffer
+  // the range's reference pair count shares the cta_begin buffer
   double* d_range_pairs = reinterpret_cast<double*>(ctx->cta_begin + nctas + 1);
-  int rc = lya_prepare_cta_ranges(ctx, nctas, ctx->cta_begin, o->slot_begin, o->slot_end, d_range_pairs);
-  if (rc != LYA_OK) return rc;
+  const int64_t n = ctx->wq.n_pairs;
+  if (ctx->cost_cap < std::max<int64_t>(n, 1)) {
+    lya_free(ctx->cost);
+    ctx->cost_cap = 0;
+    if (lya_alloc(&ctx->cost, (size_t)std::max<int64_t>(n, 1)) != cudaSuccess)
+      return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_run: allocation of the cost buffer failed");
+    ctx->cost_cap = std::max<int64_t>(n, 1);
+  }
+  size_t scan_bytes = 0;
+  if (n > 0) {
+    LYA_CHECK_CUDA(ctx, cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, ctx->cost, ctx->cost, n, s));
+    if (scan_bytes > ctx->scan_tmp_bytes) {
+      if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
+      ctx->scan_tmp = nullptr;
+      ctx->scan_tmp_bytes = 0;
+      if (cudaMalloc(&ctx->scan_tmp, scan_bytes) != cudaSuccess)
+        return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_run: allocation of the scan scratch failed");
+      ctx->scan_tmp_bytes = scan_bytes;
+    }
+  }
 
-  CorrParams p;
+  RunGraphKey key;
+  memset(&key, 0, sizeof(key));   // padding bytes take part in the comparison
+  CorrParams& p = key.p;
   const DevCatalog& c = ctx->cat;
   p.pix4 = c.pix4; p.z32 = c.z32; p.pix8 = c.pix8; p.dc = c.dc; p.w = c.w; p.dw = c.dw; p.z = c.z;
   p.pstart = c.pstart; p.len = c.len; p.sorted = c.sorted; p.slot = c.slot;
@@ -1296,31 +1353,51 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
   p.np = ctx->np; p.nt = ctx->nt; p.nb = nb;
   p.gx = (float)gx_bins; p.gy = (float)gy_bins;
   p.cos_variant = ctx->cos_variant;
-  p.run_cap = 128;
+  p.run_cap = o->run_cap > 0 ? o->run_cap : 128;
   p.variant = o->variant;
   p.hist = ctx->hist; p.counts = ctx->counts; p.stats = ctx->stats;
+  key.kind = kind; key.nctas = nctas; key.nslots = nslots; key.nb = nb; key.n_items = n;
+  key.slot_begin = o->slot_begin; key.slot_end = o->slot_end;
+  key.cost = ctx->cost; key.scan_tmp = ctx->scan_tmp; key.scan_bytes = scan_bytes;
 
-  cudaError_t e = cudaSuccess;
-  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
-  (void)warps;
-  if (kind == LYA_KERNEL_FP32_GUARDED)
-    e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16>(p, nctas, nb, s);
-  else if (kind == LYA_KERNEL_FP64_DIAGONAL)
-    e = launch_corr<LYA_KERNEL_FP64_DIAGONAL, 16>(p, nctas, nb, s);
-  else
-    e = launch_corr<LYA_KERNEL_FP64_PLAIN, 16>(p, nctas, nb, s);
-  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run launch: %s", cudaGetErrorString(e));
-  ctx->launches++;
-  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
-  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev3, s));
-  unsigned long long hst[ST_N];
-  double range_pairs = 0.0;
-  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(hst, ctx->stats, sizeof(hst), cudaMemcpyDeviceToHost, s));
-  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(&range_pairs, d_range_pairs, sizeof(double), cudaMemcpyDeviceToHost, s));
+  // shared-memory limit of the pair kernel: set outside any capture
+  {
+    cudaError_t e = cudaSuccess;
+    if (kind == LYA_KERNEL_FP32_GUARDED) e = set_corr_smem<LYA_KERNEL_FP32_GUARDED, 16>(p, nb);
+    else if (kind == LYA_KERNEL_FP64_DIAGONAL) e = set_corr_smem<LYA_KERNEL_FP64_DIAGONAL, 16>(p, nb);
+    else e = set_corr_smem<LYA_KERNEL_FP64_PLAIN, 16>(p, nb);
+    if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run: %s", cudaGetErrorString(e));
+  }
+  static_assert(sizeof(RunGraphKey) <= sizeof(ctx->run_graph_key), "graph key does not fit the context");
+  if (!ctx->run_graph || memcmp(&ctx->run_graph_key, &key, sizeof(key)) != 0) {
+    if (ctx->run_graph) { cudaGraphExecDestroy(ctx->run_graph); ctx->run_graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    LYA_CHECK_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t eq = enqueue_run(ctx, key, d_range_pairs, key.slot_begin, key.slot_end);
+    const cudaError_t ec = cudaStreamEndCapture(s, &g);
+    if (eq != cudaSuccess || ec != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run: capture failed: %s",
+                      cudaGetErrorString(eq != cudaSuccess ? eq : ec));
+    }
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run: instantiate: %s", cudaGetErrorString(ei));
+    ctx->run_graph = ex;
+    memcpy(&ctx->run_graph_key, &key, sizeof(key));
+  } else {
+    ctx->graph_launches++;
+  }
+  LYA_CHECK_CUDA(ctx, cudaGraphLaunch(ctx->run_graph, s));
+  ctx->launches += (n > 0 ? 3 : 2);   // k_item_cost (when there are items), k_cta_bounds, the pair kernel
   LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   float ms = 0.f, ms_all = 0.f;
   LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms_all, ctx->ev2, ctx->ev3));
+  const unsigned long long* hst = ctx->h_stats;
+  double range_pairs = 0.0;
+  memcpy(&range_pairs, hst + ST_N, sizeof(double));
   ctx->last.kernel_ms = ms;
   ctx->last.run_ms = ms_all;
   ctx->last.run_ref_pairs = range_pairs;
@@ -1345,6 +1422,8 @@ extern "C" int lya_corr_run(lya_ctx* ctx, const lya_corr_opts* opts) {
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: variant 3 (lean walk) exists for the FP32 kernel only");
   if (o.kernel == LYA_KERNEL_FP32_GUARDED && (size_t)2 * (ctx->np + ctx->nt) > 1024)
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: FP32 kernel needs np + nt <= 512 (threshold tables)");
+  if (o.run_cap != 0 && (o.run_cap < 8 || o.run_cap > 1024 || (o.run_cap & (o.run_cap - 1)) != 0))
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: run_cap must be 0 or a power of two in [8, 1024]");
   if (o.warps_per_block != 0 && o.warps_per_block != 16)
     return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_run: warps_per_block must be 0 or 16");
   if (o.slot_begin < 0 || o.slot_end < o.slot_begin || o.slot_end > ctx->cat.n_slots)

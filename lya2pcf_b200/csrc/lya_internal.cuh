@@ -66,6 +66,7 @@ struct DevCatalog {
 
 struct WorkQueue {
   int64_t n_pairs = 0;
+  int64_t cap = 0;             // allocated entries of f1 and f2 (reused by later queues)
   int32_t* f1 = nullptr;       // [n_pairs] grouped by f1 (non-decreasing)
   int32_t* f2 = nullptr;       // [n_pairs]
   double ref_pairs = 0.0;      // sum len1*len2
@@ -105,6 +106,17 @@ struct lya_ctx {
   int64_t* cta_begin = nullptr;          // [max ctas + 1]
   int32_t cta_cap = 0;
 
+  // persistent scratch of lya_corr_run, so a run allocates nothing once sized
+  // and its stream work can be captured in a CUDA graph and replayed
+  long long* cost = nullptr;             // [cost_cap] per-item cost, then its prefix sum
+  int64_t cost_cap = 0;
+  void* scan_tmp = nullptr;              // cub scan scratch
+  size_t scan_tmp_bytes = 0;
+  unsigned long long* h_stats = nullptr; // pinned host copy: [ST_N] counters + range pair count (as double bits)
+  cudaGraphExec_t run_graph = nullptr;   // the last run, captured
+  alignas(16) unsigned char run_graph_key[512] = {};   // what it was captured for (see corr.cu)
+  int64_t graph_launches = 0;            // runs replayed from the captured graph
+
   lya_stats_t last{};
 };
 
@@ -133,6 +145,9 @@ inline void lya_free(T*& p) {
 
 void lya_free_catalog(DevCatalog& c);
 void lya_free_queue(WorkQueue& q);
+// Room for n pairs in q (f1, f2), keeping the buffers when they are large
+// enough; n_pairs is left to the caller.
+cudaError_t lya_queue_reserve(WorkQueue& q, int64_t n);
 
 // ------------------------------------------------------------------ device math
 // cos of the angle between two lines of sight, FP64, in the contraction order
@@ -149,5 +164,4 @@ __device__ __forceinline__ double lya_cos12(double x1, double y1, double z1, dou
 int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o);
 int lya_build_queue(lya_ctx* ctx, double angmax, double mumin);
 int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int device_ptrs);
-int lya_prepare_cta_ranges(lya_ctx* ctx, int nctas, int64_t* d_out, int slot_begin, int slot_end,
-                           double* d_range_pairs);
+

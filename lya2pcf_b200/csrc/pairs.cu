@@ -229,9 +229,8 @@ int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
     cleanup();
     return lya_fail(ctx, LYA_ERR_CUDA, "lya_build_pairs: %s", cudaGetErrorString(e));
   }
-  lya_free_queue(ctx->wq);
-  e = lya_alloc(&ctx->wq.f1, (size_t)npairs);
-  if (e == cudaSuccess) e = lya_alloc(&ctx->wq.f2, (size_t)npairs);
+  ctx->wq.n_pairs = 0;
+  e = lya_queue_reserve(ctx->wq, npairs);
   if (e != cudaSuccess) {
     cleanup();
     lya_free_queue(ctx->wq);

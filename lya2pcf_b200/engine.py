@@ -46,6 +46,7 @@ class PairEngine:
         self.slot_pixels = None
         self.n_pairs = 0
         self._keep = []
+        self.tuned = {}   # kernel -> {'variant', 'run_cap'} chosen by autotune
 
     def _check(self, rc):
         N.check(rc, self.ctx)
@@ -109,13 +110,59 @@ class PairEngine:
         return f1[:self.n_pairs], f2[:self.n_pairs]
 
     # ------------------------------------------------------------------ correlation
-    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0, slots=None, variant=0):
+    def run(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, warps=0, blocks_per_sm=0, slots=None, variant=None,
+            run_cap=None):
         """Histograms of the work queue (restricted to owner slots
-        ``range(*slots)`` when given).  Returns :meth:`stats`."""
+        ``range(*slots)`` when given).  ``variant`` and ``run_cap`` default to
+        the library's defaults, or to the choice of :meth:`autotune` for this
+        kernel when it ran.  Returns :meth:`stats`."""
         s0, s1 = (0, 0) if slots is None else (int(slots[0]), int(slots[1]))
-        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), s0, s1, int(variant))
+        tuned = self.tuned.get(int(kernel), {})
+        variant = tuned.get('variant', 0) if variant is None else variant
+        run_cap = tuned.get('run_cap', 0) if run_cap is None else run_cap
+        opts = N.CorrOpts(int(kernel), float(guard), int(warps), int(blocks_per_sm), s0, s1, int(variant),
+                          int(run_cap))
         self._check(self.lib.lya_corr_run(self.ctx, C.byref(opts)))
         return self.stats()
+
+    def autotune(self, kernel=N.KERNEL_FP32_GUARDED, guard=1e-4, fraction=0.05, variants=None, run_caps=(64, 128, 256),
+                 seed=0):
+        """Choose the diagonal walk and the run-length cap of ``kernel`` for this
+        catalogue: time every candidate on a contiguous range of owner slots
+        holding about ``fraction`` of the work queue's pixel pairs (the second
+        of two runs, so each candidate is timed from its captured graph) and
+        keep the fastest for later :meth:`run` calls.  Walks: 0 (the FP32
+        kernel's lean walk, two diagonals per lane otherwise), 2 (two
+        diagonals per lane) and 1 (one per lane).  Returns the timings."""
+        if variants is None:
+            variants = (0, 2, 1) if int(kernel) == N.KERNEL_FP32_GUARDED else (0, 2)
+        slots = self._sample_slots(fraction, seed)
+        timings = []
+        for v in variants:
+            for cap in run_caps:
+                for _ in range(2):
+                    st = self.run(kernel=kernel, guard=guard, slots=slots, variant=v, run_cap=cap)
+                timings.append({'variant': v, 'run_cap': cap, 'kernel_ms': st['kernel_ms']})
+        best = min(timings, key=lambda r: r['kernel_ms'])
+        self.tuned[int(kernel)] = {'variant': best['variant'], 'run_cap': best['run_cap']}
+        return {'best': dict(self.tuned[int(kernel)]), 'slots': list(slots), 'timings': timings}
+
+    def _sample_slots(self, fraction, seed):
+        """A contiguous owner-slot range with about ``fraction`` of the queue's
+        reference pixel pairs, starting at a seeded random slot."""
+        f1, f2 = self.get_pairs()
+        L = self.fs.lengths.astype(np.float64)
+        per_slot = np.bincount(self.slot_of_forest[f1], weights=L[f1] * L[f2], minlength=len(self.slot_pixels))
+        total = per_slot.sum()
+        start = int(np.random.default_rng(seed).integers(0, max(1, len(per_slot))))
+        acc, end = 0.0, start
+        while end < len(per_slot) and acc < fraction * total:
+            acc += per_slot[end]
+            end += 1
+        while start > 0 and acc < fraction * total:   # reached the last slot: extend downwards
+            start -= 1
+            acc += per_slot[start]
+        return (start, max(end, start + 1))
 
     def timer_start(self):
         """Record a start event on the library's stream."""

@@ -194,3 +194,44 @@ def test_lean_walk_mixed_with_ineligible_forests():
         h, c = eng.histograms()
     check_hist(h, c, ho, co, N.KERNEL_FP32_GUARDED, 'lean walk with ineligible forests')
     assert c.sum() > 0
+
+
+def test_graph_replay_and_recapture(cfg0):
+    """A run is captured in a CUDA graph and replayed when called again with
+    the same options: the replay reproduces the captured run's counts bit for
+    bit; changing the walk or the run-length cap captures again and still
+    gives the same counts."""
+    fs, am, eng, _, _ = cfg0
+    eng.run(kernel=N.KERNEL_FP32_GUARDED, variant=0, run_cap=128)
+    h1, c1 = eng.histograms()
+    eng.run(kernel=N.KERNEL_FP32_GUARDED, variant=0, run_cap=128)
+    h2, c2 = eng.histograms()
+    assert np.array_equal(c1, c2)
+    np.testing.assert_allclose(h2, h1, rtol=1e-12, atol=0)
+    for var, cap in ((N.VARIANT_TWO_DIAGONALS, 64), (0, 32), (1, 256)):
+        eng.run(kernel=N.KERNEL_FP32_GUARDED, variant=var, run_cap=cap)
+        h3, c3 = eng.histograms()
+        assert np.array_equal(c3, c1), f'walk {var}, cap {cap}'
+        np.testing.assert_allclose(h3[:, N.Q_W], h1[:, N.Q_W], rtol=1e-6, atol=0)
+    # a slot-restricted run captures its own graph; the full run after it is captured again
+    eng.run(kernel=N.KERNEL_FP32_GUARDED, variant=0, run_cap=128, slots=(3, 5))
+    h4, c4 = eng.histograms()
+    assert c4[:3].sum() == 0 and c4[5:].sum() == 0 and np.array_equal(c4[3:5], c1[3:5])
+    eng.run(kernel=N.KERNEL_FP32_GUARDED, variant=0, run_cap=128)
+    h5, c5 = eng.histograms()
+    assert np.array_equal(c5, c1)
+    with pytest.raises(N.LyaError):
+        eng.run(kernel=N.KERNEL_FP32_GUARDED, run_cap=100)   # not a power of two
+
+
+def test_autotune_choice_keeps_parity(cfg0):
+    fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
+    res = eng.autotune(fraction=0.2, run_caps=(64, 128))
+    assert res['best'] in [{'variant': t['variant'], 'run_cap': t['run_cap']} for t in res['timings']]
+    assert len(res['timings']) == 6
+    ns = 4
+    ho, co = O.corr(fs, f1[:sis[ns]], f2[:sis[ns]], sis[:ns + 1])
+    eng.run()                       # the tuned walk
+    h, c = eng.histograms(0, ns)
+    check_hist(h, c, ho, co, N.KERNEL_FP32_GUARDED, 'autotuned')
+    eng.tuned.clear()
