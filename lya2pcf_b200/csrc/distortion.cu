@@ -28,11 +28,13 @@
 // rows.  Phase 2: the 50x50 (rp x rp) blocks (t, u) of D over the pair's window
 // of rt bins, diagonal blocks first (they complete the moments of bin t, read
 // from the same staged rows).  A block whose rt bins are both spanned by some
-// pixel column gets the column products as a small dense FP64 GEMM: the rows
-// of the pixels covering t and u are staged in shared memory in chunks of CH
-// pixels and every thread accumulates a TR x TC register tile; the rank-4 and
-// diagonal terms are added to the tile, and each D entry of the window gets
-// one atomic add per forest pair (both (A, B) and (B, A): D is symmetric).
+// pixel column gets the column products as a small dense FP64 GEMM on the
+// tensor cores: the rows of the pixels covering t and u are staged in shared
+// memory in chunks of CH pixels, and warp w accumulates tile row w of the
+// block (8 x 8 tiles, mma.sync m8n8k4 f64; FP64 has no tcgen05 kind); the
+// rank-4 and diagonal terms are added to the accumulators, and each D entry of
+// the window gets one atomic add per forest pair (both (A, B) and (B, A): D is
+// symmetric).
 // A forest whose sum w dl^2 is 0 has no slope to project out: its slope terms
 // are 0.
 #include <algorithm>
@@ -44,11 +46,21 @@ namespace {
 
 constexpr int DT = 256;       // threads per CTA
 constexpr int TS = 8;         // rt bins a pixel column may span
+constexpr int TSB = TS + 2;   // rows of a column being built (its window may be one bin wider at each end)
 constexpr int NW = DT / 32;   // warps per CTA
-constexpr int CH = 32;        // pixels per staged chunk of a block
-constexpr int TR = 2, TC = 5; // register tile of a thread (rp rows x rp columns)
-constexpr int NP_MAX = 64;    // np of the tiled blocks: ceil(64/2)*ceil(64/5) = 416 tiles <= 2 per thread
-constexpr int TPT = 2;        // tiles per thread
+constexpr int CH = 32;        // pixels per staged chunk of a block (a multiple of 4)
+constexpr int NP_MAX = 64;    // np of the blocks: at most 8 x 8 tiles of 8 x 8
+// Staged row length for np bins: 8 * ceil(np/8) plus 4, so the four rows of an
+// MMA fragment load fall in disjoint shared-memory banks.
+__host__ __device__ __forceinline__ int stage_npad(int np) { return 8 * ((np + 7) / 8) + 4; }
+
+// D(8x8) += A(8x4) B(4x8) in FP64 on the tensor cores (one warp).  Fragments:
+// a = A[lane/4][lane%4], b = B[lane%4][lane/4], d = D[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 struct DistParams {
   const double4* __restrict__ pix8;   // (dc, w, dw, z)
@@ -67,7 +79,7 @@ struct DistParams {
   int max_len;
   double binner_rp, binner_rt;
   int np, nt, nb, cos_variant;
-  int npad;                // staged row length (>= np, covers every tile)
+  int npad;                // staged row length (stage_npad(np))
   double* col;             // scratch [grid][2 sides][max_len][TS][np] x {S, L}
   double* D;               // [nb][nb]
   double* W;               // [nb]
@@ -75,13 +87,23 @@ struct DistParams {
   unsigned long long* next;// [1] work queue counter
 };
 
-__device__ __forceinline__ int pair_bin(double d1, double d2, double ch, double sh, const DistParams& p) {
+// Bin of a pixel pair with the reference FP64 formula, as (bp, bt); false when
+// out of range.
+__device__ __forceinline__ bool pair_bin2(double d1, double d2, double ch, double sh, const DistParams& p, int& bp,
+                                          int& bt) {
   const double rp = __dmul_rn(fabs(__dsub_rn(d1, d2)), ch);
   const double rt = __dmul_rn(__dadd_rn(d1, d2), sh);
   const double fp = floor(__dmul_rn(rp, p.binner_rp));
   const double ft = floor(__dmul_rn(rt, p.binner_rt));
-  if (fp >= 0.0 && fp < (double)p.np && ft >= 0.0 && ft < (double)p.nt) return (int)fp * p.nt + (int)ft;
-  return -1;
+  if (!(fp >= 0.0 && fp < (double)p.np && ft >= 0.0 && ft < (double)p.nt)) return false;
+  bp = (int)fp;
+  bt = (int)ft;
+  return true;
+}
+
+// rt bin coordinate floor(rt * nt / rtmax) of a pixel pair (reference formula, unclamped)
+__device__ __forceinline__ double pair_ft(double d1, double d2, double sh, const DistParams& p) {
+  return floor(__dmul_rn(__dmul_rn(__dadd_rn(d1, d2), sh), p.binner_rt));
 }
 
 __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
@@ -91,9 +113,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   double* sd = reinterpret_cast<double*>(smem);          // [2][ML] dc
   double* sw = sd + 2 * ML;                              // [2][ML] w
   double* sl = sw + 2 * ML;                              // [2][ML] dl
-  double* mom = sl + 2 * ML;                             // [4][nt][np] moments of the window's bins
+  double* ksc = sl + 2 * ML;                             // [2][ML] column-product weights k_S of a pixel
+  double* klc = ksc + 2 * ML;                            // [2][ML] and k_L
+  double* mom = klc + 2 * ML;                            // [4][nt][np] moments of the window's bins
   double* stage = mom + 4 * nt * np;                     // [4][CH][NPAD] staged rows, or the column builders
-  const int stage_len = max(4 * CH * NPAD, NW * 2 * TS * np);
+  const int stage_len = max(4 * CH * NPAD, NW * 2 * TSB * np);
   int* tlo = reinterpret_cast<int*>(stage + stage_len);  // [2][ML]
   int* span = tlo + 2 * ML;                              // [2][ML]
   int* plist = span + 2 * ML;                            // [2*ML] packed (side << 16 | pixel)
@@ -103,13 +127,14 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double* colS = p.col + (size_t)blockIdx.x * 2 * 2 * ML * TS * np;   // [2 sides][ML][TS][np]
   double* colL = colS + (size_t)2 * ML * TS * np;
-  double* myS = stage + (size_t)warp * 2 * TS * np;
-  double* myL = myS + TS * np;
+  double* myS = stage + (size_t)warp * 2 * TSB * np;
+  double* myL = myS + TSB * np;
   double* AS = stage;                  // [CH][NPAD] rows of bin t, scaled by k_S
   double* AL = AS + CH * NPAD;         // [CH][NPAD] rows of bin t, scaled by k_L
   double* BS = AL + CH * NPAD;         // [CH][NPAD] rows of bin u
   double* BL = BS + CH * NPAD;
-  const int rgroups = (np + TR - 1) / TR, cgroups = (np + TC - 1) / TC, ntiles = rgroups * cgroups;
+  const int ntile = (np + 7) / 8;   // tile rows = tile columns of a 50x50 block (7 for np = 50)
+  const int grp = lane >> 2, kq = lane & 3;
 
   for (;;) {
     if (tid == 0) s_item = (long long)atomicAdd(p.next, 1ull);
@@ -128,13 +153,18 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
     const double io2 = p.odl2[b] > 0.0 ? 1.0 / p.odl2[b] : 0.0;
     const bool srt = p.sorted[a] && p.sorted[b];
     const int64_t A0 = p.pstart[a], B0 = p.pstart[b];
+    // pixels, and the weights of their column products: an f1 pixel i enters
+    // with w_i/Om2 (S) and w_i/O2 (L), an f2 pixel j with w_j/Om1 and w_j/O1
+    const double kS1 = 1.0 / om2, kS2 = 1.0 / om1;
     for (int k = tid; k < L1; k += DT) {
       const double4 q = p.pix8[A0 + k];
       sd[k] = q.x; sw[k] = q.y; sl[k] = p.dl[A0 + k];
+      ksc[k] = q.y * kS1; klc[k] = q.y * io2;
     }
     for (int k = tid; k < L2; k += DT) {
       const double4 q = p.pix8[B0 + k];
       sd[ML + k] = q.x; sw[ML + k] = q.y; sl[ML + k] = p.dl[B0 + k];
+      ksc[ML + k] = q.y * kS2; klc[ML + k] = q.y * io1;
     }
     if (tid == 0) { s_T0 = INT_MAX; s_T1 = -1; s_maxspan = 0; }
     __syncthreads();
@@ -164,14 +194,90 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           while (x < y) { const int q = (x + y) >> 1; if (dO[q] < th) x = q + 1; else y = q; }
           jhi = x;
         }
+        // window of rt bins the column can touch, and the built rows
+        int wlo = 0, nrow = 0;
         int lo = INT_MAX, hi = -1;
-        for (int o = jlo + lane; o < jhi; o += 32) {
-          const int A = side == 0 ? pair_bin(d, dO[o], ch, sh, p) : pair_bin(dO[o], d, ch, sh, p);
-          if (A >= 0) { const int bt = A % nt; lo = min(lo, bt); hi = max(hi, bt); }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-          lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-          hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        if (srt) {
+          // sorted: the rt bin is non-decreasing in the partner index, so the
+          // partners at the two ends of the range bound the window; one pass,
+          // each lane over a contiguous segment of partners, equal-bin runs
+          // merged in registers before the shared-memory add
+          if (jlo < jhi) {
+            const double f0 = side == 0 ? pair_ft(d, dO[jlo], sh, p) : pair_ft(dO[jlo], d, sh, p);
+            const double f1v = side == 0 ? pair_ft(d, dO[jhi - 1], sh, p) : pair_ft(dO[jhi - 1], d, sh, p);
+            const double flo = fmax(f0, 0.0), fhi = fmin(f1v, (double)(nt - 1));
+            if (flo <= fhi) {
+              wlo = (int)flo;
+              nrow = (int)fhi - wlo + 1;
+            }
+          }
+          if (nrow > TSB) {
+            if (lane == 0) atomicAdd(p.err, 1ull);
+            nrow = 0;
+          }
+          if (nrow > 0) {
+            for (int q = lane; q < nrow * np; q += 32) { myS[q] = 0.0; myL[q] = 0.0; }
+            __syncwarp();
+            const int cnt = jhi - jlo, seg = (cnt + 31) / 32;
+            int j = jlo + lane * seg;
+            const int je = min(jhi, j + seg);
+            int cbp = -1, cbt = -1;
+            double as = 0.0, al = 0.0;
+            for (; j < je; ++j) {
+              int bp, bt;
+              const bool in = side == 0 ? pair_bin2(d, dO[j], ch, sh, p, bp, bt) : pair_bin2(dO[j], d, ch, sh, p, bp, bt);
+              if (!in) { bp = -1; bt = -1; }
+              if (bp != cbp || bt != cbt) {
+                if (cbp >= 0) {
+                  const int q = (cbt - wlo) * np + cbp;
+                  atomicAdd(&myS[q], as);
+                  atomicAdd(&myL[q], al);
+                }
+                cbp = bp; cbt = bt; as = 0.0; al = 0.0;
+              }
+              if (in) {
+                as += wO[j];
+                al = fma(wO[j], lO[j], al);
+                lo = min(lo, bt);
+                hi = max(hi, bt);
+              }
+            }
+            if (cbp >= 0) {
+              const int q = (cbt - wlo) * np + cbp;
+              atomicAdd(&myS[q], as);
+              atomicAdd(&myL[q], al);
+            }
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+          }
+        } else {
+          // unsorted: a first pass finds the rt bins the column touches
+          for (int o = jlo + lane; o < jhi; o += 32) {
+            int bp, bt;
+            const bool in = side == 0 ? pair_bin2(d, dO[o], ch, sh, p, bp, bt) : pair_bin2(dO[o], d, ch, sh, p, bp, bt);
+            if (in) { lo = min(lo, bt); hi = max(hi, bt); }
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+          }
+          if (hi >= lo && hi - lo + 1 <= TS) {
+            wlo = lo;
+            nrow = hi - lo + 1;
+            for (int q = lane; q < nrow * np; q += 32) { myS[q] = 0.0; myL[q] = 0.0; }
+            __syncwarp();
+            for (int o = jlo + lane; o < jhi; o += 32) {
+              int bp, bt;
+              const bool in = side == 0 ? pair_bin2(d, dO[o], ch, sh, p, bp, bt) : pair_bin2(dO[o], d, ch, sh, p, bp, bt);
+              if (in) {
+                const int q = (bt - wlo) * np + bp;
+                atomicAdd(&myS[q], wO[o]);
+                atomicAdd(&myL[q], wO[o] * lO[o]);
+              }
+            }
+          }
         }
         int sp = hi >= lo ? hi - lo + 1 : 0;
         if (sp > TS) {
@@ -182,29 +288,20 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           tlo[side * ML + m] = lo;
           span[side * ML + m] = sp;
         }
+        __syncwarp();
         if (sp > 0) {
-          for (int q = lane; q < sp * np; q += 32) { myS[q] = 0.0; myL[q] = 0.0; }
-          __syncwarp();
-          for (int o = jlo + lane; o < jhi; o += 32) {
-            const int A = side == 0 ? pair_bin(d, dO[o], ch, sh, p) : pair_bin(dO[o], d, ch, sh, p);
-            if (A >= 0) {
-              const int bp = A / nt, bt = A - bp * nt;
-              const int q = (bt - lo) * np + bp;
-              atomicAdd(&myS[q], wO[o]);
-              atomicAdd(&myL[q], wO[o] * lO[o]);
-            }
-          }
-          __syncwarp();
+          // rows lo..hi of the built window go to the CTA's scratch
           double* rs = cS + (size_t)m * TS * np;
           double* rl = cL + (size_t)m * TS * np;
-          for (int q = lane; q < sp * np; q += 32) { rs[q] = myS[q]; rl[q] = myL[q]; }
+          const int off = (lo - wlo) * np;
+          for (int q = lane; q < sp * np; q += 32) { rs[q] = myS[off + q]; rl[q] = myL[off + q]; }
           if (lane == 0) {
             atomicMin(&s_T0, lo);
             atomicMax(&s_T1, lo + sp - 1);
             atomicMax(&s_maxspan, sp);
           }
-          __syncwarp();
         }
+        __syncwarp();
       }
     }
     __syncthreads();
@@ -230,11 +327,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         while (r >= nT - 1 - tt) { r -= nT - 1 - tt; ++tt; }
         t = T0 + tt; u = t + 1 + r;
       }
-      double acc[TPT][TR * TC];
+      // warp w < ntile owns tile row w (bp = 8w + lane/4): one accumulator
+      // fragment per tile column (bq = 8c + 2(lane%4) + {0,1})
+      double acc[8][2];
 #pragma unroll
-      for (int k = 0; k < TPT; ++k)
-#pragma unroll
-        for (int q = 0; q < TR * TC; ++q) acc[k][q] = 0.0;
+      for (int c = 0; c < 8; ++c) { acc[c][0] = 0.0; acc[c][1] = 0.0; }
       if (u - t < maxspan) {
         // pixels whose column spans both t and u
         if (tid == 0) s_cnt = 0;
@@ -250,23 +347,31 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         const int n = s_cnt;
         for (int c0 = 0; c0 < n; c0 += CH) {
           const int rows = min(CH, n - c0);
-          for (int e = tid; e < rows * NPAD; e += DT) {
-            const int r = e / NPAD, bq = e - r * NPAD;
-            const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
-            double vs = 0.0, vl = 0.0, us = 0.0, ul = 0.0;
-            if (bq < np) {
+          const int rows4 = (rows + 3) & ~3;   // MMA steps take 4 rows; the padding rows are zero
+          for (int r = warp; r < rows4; r += NW) {   // a warp per staged row, lanes over the bins
+            const double *cs = nullptr, *cl = nullptr;
+            double kS = 0.0, kL = 0.0;
+            int ot = 0, ou = 0;
+            if (r < rows) {
+              const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
               const int lo = tlo[side * ML + m];
-              const double* cs = colS + (size_t)side * ML * TS * np + (size_t)m * TS * np;
-              const double* cl = colL + (size_t)side * ML * TS * np + (size_t)m * TS * np;
-              const double wm = sw[side * ML + m];
-              const double kS = side == 0 ? wm / om2 : wm / om1;
-              const double kL = side == 0 ? wm * io2 : wm * io1;
-              vs = kS * cs[(t - lo) * np + bq];
-              vl = kL * cl[(t - lo) * np + bq];
-              us = cs[(u - lo) * np + bq];
-              ul = cl[(u - lo) * np + bq];
+              cs = colS + (size_t)side * ML * TS * np + (size_t)m * TS * np;
+              cl = colL + (size_t)side * ML * TS * np + (size_t)m * TS * np;
+              kS = ksc[side * ML + m];
+              kL = klc[side * ML + m];
+              ot = (t - lo) * np;
+              ou = (u - lo) * np;
             }
-            AS[r * NPAD + bq] = vs; AL[r * NPAD + bq] = vl; BS[r * NPAD + bq] = us; BL[r * NPAD + bq] = ul;
+            for (int bq = lane; bq < NPAD; bq += 32) {
+              double vs = 0.0, vl = 0.0, us = 0.0, ul = 0.0;
+              if (r < rows && bq < np) {
+                vs = kS * cs[ot + bq];
+                vl = kL * cl[ot + bq];
+                us = cs[ou + bq];
+                ul = cl[ou + bq];
+              }
+              AS[r * NPAD + bq] = vs; AL[r * NPAD + bq] = vl; BS[r * NPAD + bq] = us; BL[r * NPAD + bq] = ul;
+            }
           }
           __syncthreads();
           if (t == u) {   // moments of bin t from the unscaled rows of the f1 pixels
@@ -284,45 +389,38 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
               mom[(q * nt + t) * np + bq] += sacc;
             }
           }
+          if (warp < ntile) {
+            for (int r0 = 0; r0 < rows4; r0 += 4) {
+              const int ra = (r0 + kq) * NPAD;
+              const double as = AS[ra + 8 * warp + grp], al = AL[ra + 8 * warp + grp];
 #pragma unroll
-          for (int k = 0; k < TPT; ++k) {
-            const int tile = tid + k * DT;
-            if (tile < ntiles) {
-              const int r0 = (tile / cgroups) * TR, q0 = (tile % cgroups) * TC;
-              for (int r = 0; r < rows; ++r) {
-                const double* as = AS + r * NPAD + r0;
-                const double* bs = BS + r * NPAD + q0;
-                const double* al = AL + r * NPAD + r0;
-                const double* bl = BL + r * NPAD + q0;
-#pragma unroll
-                for (int i = 0; i < TR; ++i)
-#pragma unroll
-                  for (int j = 0; j < TC; ++j) acc[k][i * TC + j] = fma(as[i], bs[j], fma(al[i], bl[j], acc[k][i * TC + j]));
+              for (int c = 0; c < 8; ++c) {
+                if (c < ntile) {
+                  dmma_8x8x4(acc[c][0], acc[c][1], as, BS[ra + 8 * c + grp]);
+                  dmma_8x8x4(acc[c][0], acc[c][1], al, BL[ra + 8 * c + grp]);
+                }
               }
             }
           }
           __syncthreads();
         }
       }
-      // flush: column products (subtracted), rank-4 part, diagonal
+      // flush: column products (subtracted), rank-4 part, diagonal; warp w
+      // writes tile row w, lane (grp, kq) the entries (8w + grp, 8c + 2kq + i)
+      if (warp < ntile) {
+        const int bp = 8 * warp + grp;
+        if (bp < np) {
+          const double* mt = mom + (size_t)t * np + bp;   // + q*nt*np
+          const double m0a = mt[0], mia = mt[nt * np], mja = mt[2 * nt * np], mija = mt[3 * nt * np];
 #pragma unroll
-      for (int k = 0; k < TPT; ++k) {
-        const int tile = tid + k * DT;
-        if (tile < ntiles) {
-          const int r0 = (tile / cgroups) * TR, q0 = (tile % cgroups) * TC;
+          for (int c = 0; c < 8; ++c) {
 #pragma unroll
-          for (int i = 0; i < TR; ++i) {
-            const int bp = r0 + i;
-            if (bp >= np) continue;
-            const double* mt = mom + (size_t)t * np + bp;   // + q*nt*np
-            const double m0a = mt[0], mia = mt[nt * np], mja = mt[2 * nt * np], mija = mt[3 * nt * np];
-#pragma unroll
-            for (int j = 0; j < TC; ++j) {
-              const int bq = q0 + j;
-              if (bq >= np) continue;
+            for (int i = 0; i < 2; ++i) {
+              const int bq = 8 * c + 2 * kq + i;
+              if (c >= ntile || bq >= np) continue;
               const double* mu = mom + (size_t)u * np + bq;
               double v = m0a * mu[0] * cA + mja * mu[2 * nt * np] * cB + mia * mu[nt * np] * cC +
-                         mija * mu[3 * nt * np] * cD - acc[k][i * TC + j];
+                         mija * mu[3 * nt * np] * cD - acc[c][i];
               const int A = bp * nt + t, B = bq * nt + u;
               if (A == B) {
                 v += m0a;
@@ -356,9 +454,9 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   for (int64_t f = 0; f < ctx->cat.n; ++f)
     max_len = std::max<int>(max_len, (int)(ctx->h_start[f + 1] - ctx->h_start[f]));
   if (max_len > 65535) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests longer than 65535 pixels");
-  const int npad = std::max(TR * ((np + TR - 1) / TR), TC * ((np + TC - 1) / TC));
-  const size_t stage_len = std::max<size_t>((size_t)4 * CH * npad, (size_t)NW * 2 * TS * np);
-  const size_t smem = sizeof(double) * (6 * (size_t)max_len + 4 * (size_t)nt * np + stage_len) +
+  const int npad = stage_npad(np);
+  const size_t stage_len = std::max<size_t>((size_t)4 * CH * npad, (size_t)NW * 2 * TSB * np);
+  const size_t smem = sizeof(double) * (10 * (size_t)max_len + 4 * (size_t)nt * np + stage_len) +
                       sizeof(int) * (6 * (size_t)max_len);
   if (smem > 227 * 1024)
     return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory", max_len, smem);
