@@ -263,12 +263,17 @@ extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start,
     ctx->launches++;
     e = cudaGetLastError();
   }
+  // forests the FP32 kernel's lean walk cannot take (they need the second pass)
+  std::vector<uint8_t> flags((size_t)n);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(flags.data(), c.sorted, (size_t)n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cleanup_tmp();
   if (e != cudaSuccess) {
     lya_free_catalog(ctx->cat);
     return lya_fail(ctx, LYA_ERR_CUDA, "lya_upload_forests: %s", cudaGetErrorString(e));
   }
+  c.n_not_lean = 0;
+  for (int64_t f = 0; f < n; ++f) c.n_not_lean += (flags[f] & LYA_LEAN) ? 0 : 1;
   return LYA_OK;
 }
 

@@ -1054,7 +1054,15 @@ constexpr size_t rec_bytes() {
   return KIND == LYA_KERNEL_FP32_GUARDED ? sizeof(RecF32) : (KIND == LYA_KERNEL_FP64_DIAGONAL ? sizeof(RecF64) : 0);
 }
 
-template <int KIND, int WARPS>
+// Walk selection of a pair-kernel instance.  The FP32 kernel runs as one
+// instance with the lean walk only (pairs of two lean forests; the others are
+// skipped) followed, when the catalogue has forests the lean walk cannot take,
+// by one with the two-diagonal walk for exactly those pairs, so each instance
+// carries one walk's code; WALK_ANY takes every pair with the walk
+// p.variant names.
+enum { WALK_ANY = 0, WALK_LEAN = 1, WALK_REST = 2 };
+
+template <int KIND, int WARPS, int WALK>
 __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int nb = p.nb;
@@ -1102,10 +1110,17 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
       t = __shfl_sync(FULL, t, 0);
       if ((int64_t)t >= seg_end) break;
       if (KIND == LYA_KERNEL_FP32_GUARDED) {
-        if (p.variant == 1) item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
-        else if (p.variant != 2 && (p.sorted[p.f1[t]] & p.sorted[p.f2[t]] & LYA_LEAN))
-          item_lean(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), myctl, cnt, st);
-        else item_diag2<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+        if (WALK == WALK_LEAN) {
+          if (p.sorted[p.f1[t]] & p.sorted[p.f2[t]] & LYA_LEAN)
+            item_lean(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), myctl, cnt, st);
+        } else if (WALK == WALK_REST) {
+          if (!(p.sorted[p.f1[t]] & p.sorted[p.f2[t]] & LYA_LEAN))
+            item_diag2<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+        } else if (p.variant == 1) {
+          item_diag<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+        } else {
+          item_diag2<TrF32, true>(p, (int64_t)t, h, reinterpret_cast<RecF32*>(mybuf), cnt, st);
+        }
       } else if (KIND == LYA_KERNEL_FP64_DIAGONAL) {
         if (p.variant == 2) item_diag2<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
         else item_diag<TrF64, false>(p, (int64_t)t, h, reinterpret_cast<RecF64*>(mybuf), cnt, st);
@@ -1160,17 +1175,21 @@ size_t corr_smem_bytes(const CorrParams& p, int nb) {
          (KIND == LYA_KERNEL_FP32_GUARDED ? (size_t)WARPS * lean_ctl_stride(p.np, p.nt) * sizeof(float) : 0);
 }
 
-template <int KIND, int WARPS>
+template <int KIND, int WARPS, int WALK>
 cudaError_t set_corr_smem(const CorrParams& p, int nb) {
-  return cudaFuncSetAttribute(k_corr<KIND, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_corr<KIND, WARPS, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)corr_smem_bytes<KIND, WARPS>(p, nb));
 }
 
-template <int KIND, int WARPS>
+template <int KIND, int WARPS, int WALK>
 cudaError_t launch_corr(const CorrParams& p, int nctas, int nb, cudaStream_t s) {
-  k_corr<KIND, WARPS><<<nctas, WARPS * 32, corr_smem_bytes<KIND, WARPS>(p, nb), s>>>(p);
+  k_corr<KIND, WARPS, WALK><<<nctas, WARPS * 32, corr_smem_bytes<KIND, WARPS>(p, nb), s>>>(p);
   return cudaGetLastError();
 }
+
+// The FP32 kernel's default walk: the lean instance, plus the two-diagonal
+// instance for the pairs it skips when the catalogue has forests it cannot take.
+static bool fp32_lean_walk(int variant) { return variant == 0 || variant == 3; }
 
 // ------------------------------------------------------------------ CTA ranges
 __global__ void k_item_cost(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ f2,
@@ -1233,6 +1252,7 @@ struct RunGraphKey {
   CorrParams p;
   int kind, nctas, nslots, nb;
   int slot_begin, slot_end;
+  int rest_pass;          // FP32 lean walk: second instance for the pairs it skips
   int64_t n_items;
   const void* cost;
   const void* scan_tmp;
@@ -1267,9 +1287,16 @@ static cudaError_t enqueue_run(lya_ctx* ctx, const RunGraphKey& k, double* d_ran
   }
   if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev0, s, cudaEventRecordExternal);
   if (e == cudaSuccess) {
-    if (k.kind == LYA_KERNEL_FP32_GUARDED) e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16>(p, k.nctas, k.nb, s);
-    else if (k.kind == LYA_KERNEL_FP64_DIAGONAL) e = launch_corr<LYA_KERNEL_FP64_DIAGONAL, 16>(p, k.nctas, k.nb, s);
-    else e = launch_corr<LYA_KERNEL_FP64_PLAIN, 16>(p, k.nctas, k.nb, s);
+    if (k.kind == LYA_KERNEL_FP32_GUARDED && fp32_lean_walk(p.variant)) {
+      e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16, WALK_LEAN>(p, k.nctas, k.nb, s);
+      if (e == cudaSuccess && k.rest_pass) e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16, WALK_REST>(p, k.nctas, k.nb, s);
+    } else if (k.kind == LYA_KERNEL_FP32_GUARDED) {
+      e = launch_corr<LYA_KERNEL_FP32_GUARDED, 16, WALK_ANY>(p, k.nctas, k.nb, s);
+    } else if (k.kind == LYA_KERNEL_FP64_DIAGONAL) {
+      e = launch_corr<LYA_KERNEL_FP64_DIAGONAL, 16, WALK_ANY>(p, k.nctas, k.nb, s);
+    } else {
+      e = launch_corr<LYA_KERNEL_FP64_PLAIN, 16, WALK_ANY>(p, k.nctas, k.nb, s);
+    }
   }
   if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev1, s, cudaEventRecordExternal);
   if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev3, s, cudaEventRecordExternal);
@@ -1358,14 +1385,21 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
   p.hist = ctx->hist; p.counts = ctx->counts; p.stats = ctx->stats;
   key.kind = kind; key.nctas = nctas; key.nslots = nslots; key.nb = nb; key.n_items = n;
   key.slot_begin = o->slot_begin; key.slot_end = o->slot_end;
+  key.rest_pass = (kind == LYA_KERNEL_FP32_GUARDED && fp32_lean_walk(o->variant) && ctx->cat.n_not_lean > 0) ? 1 : 0;
   key.cost = ctx->cost; key.scan_tmp = ctx->scan_tmp; key.scan_bytes = scan_bytes;
 
   // shared-memory limit of the pair kernel: set outside any capture
   {
     cudaError_t e = cudaSuccess;
-    if (kind == LYA_KERNEL_FP32_GUARDED) e = set_corr_smem<LYA_KERNEL_FP32_GUARDED, 16>(p, nb);
-    else if (kind == LYA_KERNEL_FP64_DIAGONAL) e = set_corr_smem<LYA_KERNEL_FP64_DIAGONAL, 16>(p, nb);
-    else e = set_corr_smem<LYA_KERNEL_FP64_PLAIN, 16>(p, nb);
+    if (kind == LYA_KERNEL_FP32_GUARDED) {
+      e = set_corr_smem<LYA_KERNEL_FP32_GUARDED, 16, WALK_LEAN>(p, nb);
+      if (e == cudaSuccess) e = set_corr_smem<LYA_KERNEL_FP32_GUARDED, 16, WALK_REST>(p, nb);
+      if (e == cudaSuccess) e = set_corr_smem<LYA_KERNEL_FP32_GUARDED, 16, WALK_ANY>(p, nb);
+    } else if (kind == LYA_KERNEL_FP64_DIAGONAL) {
+      e = set_corr_smem<LYA_KERNEL_FP64_DIAGONAL, 16, WALK_ANY>(p, nb);
+    } else {
+      e = set_corr_smem<LYA_KERNEL_FP64_PLAIN, 16, WALK_ANY>(p, nb);
+    }
     if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_run: %s", cudaGetErrorString(e));
   }
   static_assert(sizeof(RunGraphKey) <= sizeof(ctx->run_graph_key), "graph key does not fit the context");
@@ -1390,7 +1424,8 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
     ctx->graph_launches++;
   }
   LYA_CHECK_CUDA(ctx, cudaGraphLaunch(ctx->run_graph, s));
-  ctx->launches += (n > 0 ? 3 : 2);   // k_item_cost (when there are items), k_cta_bounds, the pair kernel
+  // k_item_cost (when there are items), k_cta_bounds, the pair kernel (two instances with the rest pass)
+  ctx->launches += (n > 0 ? 3 : 2) + key.rest_pass;
   LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   float ms = 0.f, ms_all = 0.f;
   LYA_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));

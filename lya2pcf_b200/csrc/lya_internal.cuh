@@ -62,6 +62,7 @@ struct DevCatalog {
   float* z32 = nullptr;
   bool has_dl = false;
   bool has_moments = false;
+  int64_t n_not_lean = 0;      // forests without the LYA_LEAN flag
 };
 
 struct WorkQueue {
