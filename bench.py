@@ -56,6 +56,7 @@ def parse():
     ap.add_argument('--dist-scale', type=float, default=0.03,
                     help='distortion sample: fraction of the 30,000-forest distortion catalogue (0 = skip)')
     ap.add_argument('--no-adjoint', action='store_true', help='skip the adjoint timing')
+    ap.add_argument('--no-covariance', action='store_true', help='skip the covariance post-processing timing')
     return ap.parse_args()
 
 
@@ -318,6 +319,21 @@ def run_b200(args, dist):
         e2e_s = dist.max(time.perf_counter() - t)
         e2e_value = dist.sum(ref_pairs * args.e2e_steps) / e2e_s
 
+    # ---- covariance of the per-owner-pixel correlations of the last run (post-processing, on the device)
+    covariance = None
+    if not args.no_covariance:
+        try:
+            t = time.perf_counter()
+            mean, cmat, csm, smoothed = eng.covariance()
+            cov_s = time.perf_counter() - t
+            covariance = {'seconds': cov_s, 'gram_kernels_ms': eng.stats()['kernel_ms'], 'rows': len(slot_pixels),
+                          'bins': eng.nb, 'smoothed': smoothed,
+                          'gram_fma': float(len(slot_pixels)) * eng.nb * eng.nb,
+                          'what': 'lya_covariance (rows from the run on the device, FP64 tensor-core Gram) + '
+                                  'lya_covariance_smooth, wall clock with the 50 MB copies out'}
+        except N.LyaError as err:
+            covariance = {'error': str(err)}
+
     # ---- adjoint (gradient of sum_b g_b DW_b/W_b w.r.t. dw and w of every pixel) on the same catalogue
     adjoint = None
     if not args.no_adjoint:
@@ -369,7 +385,7 @@ def run_b200(args, dist):
                'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                        'path': 'lya_upload_forests + lya_build_pairs + lya_corr_run + lya_corr_get, pinned host'},
                'tuned': tune, 'kernel_ms_steps': kernel_ms, 'run_ms_steps': run_ms, 'build_ms_steps': build_ms,
-               'distortion': distortion, 'adjoint': adjoint,
+               'distortion': distortion, 'adjoint': adjoint, 'covariance': covariance,
                'gpu_launches': int(launches),
                'kernel_ms': kms, 'build_ms': float(np.median(build_ms)),
                'evaluated_pairs_per_step': st['evaluated_pairs'], 'guard_rechecks_per_step': st['guard_rechecks'],

@@ -153,6 +153,26 @@ int lya_dist_run(lya_ctx* ctx, double* D, double* W);
 
 int lya_stats(lya_ctx* ctx, lya_stats_t* out);
 
+/* Covariance of the per-pixel correlation estimates; replaces cov
+ * (post_processing.py:30-52), fed by the reading loop of post_processing.py:
+ * 134-149.  xi and w are host arrays [n_rows][np*nt] (xi = DW/W of an owner
+ * pixel, 0 where W = 0, and w = W, in bin_coordinates order: bin p*nt + t,
+ * post_processing.py:13-28); with xi and w both NULL the rows are the owner
+ * slots of the last lya_corr_run, read on the device (n_rows is ignored).
+ * Outputs (host, either may be NULL): mean[np*nt] (the weighted mean
+ * correlation) and cov[np*nt][np*nt]; the covariance is also kept on the
+ * device for lya_covariance_smooth.  A bin whose weights sum to 0 is
+ * LYA_ERR_DATA (the reference's numba code raises ZeroDivisionError). */
+int lya_covariance(lya_ctx* ctx, int64_t n_rows, const double* xi, const double* w, double* mean, double* cov);
+
+/* Smoothed covariance; replaces cov_smooth (post_processing.py:54-91): the
+ * correlation matrix averaged over pairs of bins with equal (|r_par step|,
+ * |r_perp step|), scaled back by sqrt(C_aa C_bb).  cov is a host matrix
+ * [np*nt][np*nt], or NULL for the one the last lya_covariance kept.  When a
+ * variance is 0 the output is the unsmoothed covariance and *smoothed = 0, as
+ * the reference returns it. */
+int lya_covariance_smooth(lya_ctx* ctx, const double* cov, double* cov_smooth, int32_t* smoothed);
+
 /* Histograms of one owner pixel without any device allocation.  No
  * counterpart in the reference.  For callers that cannot allocate device
  * memory (device memory owned by another framework's caching allocator, a

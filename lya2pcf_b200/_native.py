@@ -42,6 +42,8 @@ SIGNATURES = {
     'lya_timer': ([P, C.c_int32, C.POINTER(C.c_double)], C.c_int),
     'lya_dist_run': ([P, P, P], C.c_int),
     'lya_sync': ([P], C.c_int),
+    'lya_covariance': ([P, C.c_int64, P, P, P, P], C.c_int),
+    'lya_covariance_smooth': ([P, P, P, C.POINTER(C.c_int32)], C.c_int),
     'lya_corr_pixel_noalloc': ([C.c_int, P, P, P, P, P, P, P, P, P, P, C.c_int64, C.c_double, C.c_double,
                                 C.c_int32, C.c_int32, P, P, P], C.c_int),
 }

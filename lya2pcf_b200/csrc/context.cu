@@ -105,6 +105,7 @@ extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
   lya_free_queue(ctx->wq);
   lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
   lya_free(ctx->cost);
+  lya_free(ctx->cov);
   if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
   if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
   if (ctx->run_graph) cudaGraphExecDestroy(ctx->run_graph);

@@ -54,14 +54,6 @@ constexpr int NP_MAX = 64;    // np of the blocks: at most 8 x 8 tiles of 8 x 8
 // MMA fragment load fall in disjoint shared-memory banks.
 __host__ __device__ __forceinline__ int stage_npad(int np) { return 8 * ((np + 7) / 8) + 4; }
 
-// D(8x8) += A(8x4) B(4x8) in FP64 on the tensor cores (one warp).  Fragments:
-// a = A[lane/4][lane%4], b = B[lane%4][lane/4], d = D[lane/4][2*(lane%4) + {0,1}].
-__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
 struct DistParams {
   const double4* __restrict__ pix8;   // (dc, w, dw, z)
   const double* __restrict__ dl;
@@ -396,8 +388,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
 #pragma unroll
               for (int c = 0; c < 8; ++c) {
                 if (c < ntile) {
-                  dmma_8x8x4(acc[c][0], acc[c][1], as, BS[ra + 8 * c + grp]);
-                  dmma_8x8x4(acc[c][0], acc[c][1], al, BL[ra + 8 * c + grp]);
+                  lya_dmma_8x8x4(acc[c][0], acc[c][1], as, BS[ra + 8 * c + grp]);
+                  lya_dmma_8x8x4(acc[c][0], acc[c][1], al, BL[ra + 8 * c + grp]);
                 }
               }
             }

@@ -119,6 +119,11 @@ struct lya_ctx {
   int64_t graph_launches = 0;            // runs replayed from the captured graph
 
   lya_stats_t last{};
+
+  // covariance post-processing: the last covariance, kept for lya_covariance_smooth
+  double* cov = nullptr;                 // [cov_nb][cov_nb]
+  int32_t cov_nb = 0;
+  bool have_cov = false;
 };
 
 // ------------------------------------------------------------------ errors
@@ -159,6 +164,15 @@ __device__ __forceinline__ double lya_cos12(double x1, double y1, double z1, dou
   if (variant == 0) return __fma_rn(z1, z2, __fma_rn(x1, x2, __dmul_rn(y1, y2)));
   if (variant == 1) return __fma_rn(z1, z2, __fma_rn(y1, y2, __dmul_rn(x1, x2)));
   return __dadd_rn(__dadd_rn(__dmul_rn(x1, x2), __dmul_rn(y1, y2)), __dmul_rn(z1, z2));
+}
+
+// D(8x8) += A(8x4) B(4x8) in FP64 on the tensor cores, one warp (FP64 has no
+// tcgen05 kind).  Fragments: a = A[lane/4][lane%4], b = B[lane%4][lane/4],
+// d = D[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void lya_dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
 }
 
 // ------------------------------------------------------------------ launchers

@@ -222,6 +222,21 @@ class PairEngine:
         self._check(self.lib.lya_dist_run(self.ctx, N.ptr(D), N.ptr(W)))
         return D, W
 
+    def covariance(self, smooth=True):
+        """Covariance of the per-owner-slot correlation estimates xi = DW/W of
+        the last :meth:`run`, computed on the device from its histograms (the
+        reading loop and ``cov``/``cov_smooth`` of ``post_processing.py``).
+        Returns ``(mean[nb], cov[nb, nb], cov_smooth[nb, nb] or None, smoothed)``."""
+        mean = np.zeros(self.nb)
+        c = np.zeros((self.nb, self.nb))
+        self._check(self.lib.lya_covariance(self.ctx, 0, None, None, N.ptr(mean), N.ptr(c)))
+        if not smooth:
+            return mean, c, None, False
+        cs = np.zeros_like(c)
+        sm = C.c_int32(0)
+        self._check(self.lib.lya_covariance_smooth(self.ctx, None, N.ptr(cs), C.byref(sm)))
+        return mean, c, cs, bool(sm.value)
+
     def stats(self):
         st = N.Stats()
         self._check(self.lib.lya_stats(self.ctx, C.byref(st)))
