@@ -44,7 +44,7 @@
 
 namespace {
 
-constexpr int DT = 256;       // threads per CTA
+constexpr int DT = 512;       // threads per CTA
 constexpr int TS = 8;         // rt bins a pixel column may span
 constexpr int TSB = TS + 2;   // rows of a column being built (its window may be one bin wider at each end)
 constexpr int NW = DT / 32;   // warps per CTA
@@ -73,6 +73,7 @@ struct DistParams {
   int np, nt, nb, cos_variant;
   int npad;                // staged row length (stage_npad(np))
   double* col;             // scratch [grid][2 sides][max_len][TS][np] x {S, L}
+  double* moments;         // scratch [grid][4][nt][np]: moments of the window's bins
   double* D;               // [nb][nb]
   double* W;               // [nb]
   unsigned long long* err; // [1] pixels whose column spans more than TS rt bins
@@ -107,8 +108,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   double* sl = sw + 2 * ML;                              // [2][ML] dl
   double* ksc = sl + 2 * ML;                             // [2][ML] column-product weights k_S of a pixel
   double* klc = ksc + 2 * ML;                            // [2][ML] and k_L
-  double* mom = klc + 2 * ML;                            // [4][nt][np] moments of the window's bins
-  double* stage = mom + 4 * nt * np;                     // [4][CH][NPAD] staged rows, or the column builders
+  double* mom = p.moments + (size_t)blockIdx.x * 4 * nt * np;   // [4][nt][np] (CTA-private, L2-resident)
+  double* stage = klc + 2 * ML;                          // [4][CH][NPAD] staged rows, or the column builders
   const int stage_len = max(4 * CH * NPAD, NW * 2 * TSB * np);
   int* tlo = reinterpret_cast<int*>(stage + stage_len);  // [2][ML]
   int* span = tlo + 2 * ML;                              // [2][ML]
@@ -448,18 +449,19 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   if (max_len > 65535) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests longer than 65535 pixels");
   const int npad = stage_npad(np);
   const size_t stage_len = std::max<size_t>((size_t)4 * CH * npad, (size_t)NW * 2 * TSB * np);
-  const size_t smem = sizeof(double) * (10 * (size_t)max_len + 4 * (size_t)nt * np + stage_len) +
+  const size_t smem = sizeof(double) * (10 * (size_t)max_len + stage_len) +
                       sizeof(int) * (6 * (size_t)max_len);
   if (smem > 227 * 1024)
     return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory", max_len, smem);
   const int grid = ctx->num_sms;
-  double *d_D = nullptr, *d_W = nullptr, *col = nullptr;
+  double *d_D = nullptr, *d_W = nullptr, *col = nullptr, *moments = nullptr;
   unsigned long long* err = nullptr;
   cudaError_t e = lya_alloc(&d_D, (size_t)nb * nb);
   if (e == cudaSuccess) e = lya_alloc(&d_W, nb);
   if (e == cudaSuccess) e = lya_alloc(&col, (size_t)grid * 2 * 2 * max_len * TS * np);
+  if (e == cudaSuccess) e = lya_alloc(&moments, (size_t)grid * 4 * nt * np);
   if (e == cudaSuccess) e = lya_alloc(&err, 2);
-  auto cleanup = [&]() { lya_free(d_D); lya_free(d_W); lya_free(col); lya_free(err); };
+  auto cleanup = [&]() { lya_free(d_D); lya_free(d_W); lya_free(col); lya_free(moments); lya_free(err); };
   if (e != cudaSuccess) {
     cleanup();
     return lya_fail(ctx, LYA_ERR_ALLOC, "lya_dist_run: device allocation failed");
@@ -477,7 +479,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     p.n_items = ctx->wq.n_pairs; p.max_len = max_len;
     p.binner_rp = (double)np / ctx->rpmax; p.binner_rt = (double)nt / ctx->rtmax;
     p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant; p.npad = npad;
-    p.col = col; p.D = d_D; p.W = d_W; p.err = err; p.next = err + 1;
+    p.col = col; p.moments = moments; p.D = d_D; p.W = d_W; p.err = err; p.next = err + 1;
     e = cudaFuncSetAttribute(k_dist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) {
       k_dist<<<grid, DT, smem, s>>>(p);
