@@ -106,6 +106,9 @@ extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
   lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
   lya_free(ctx->cost);
   lya_free(ctx->cov);
+  lya_free(ctx->dist.D); lya_free(ctx->dist.W); lya_free(ctx->dist.col); lya_free(ctx->dist.mom);
+  lya_free(ctx->dist.err);
+  if (ctx->dist.graph) cudaGraphExecDestroy(ctx->dist.graph);
   if (ctx->scan_tmp) cudaFree(ctx->scan_tmp);
   if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
   if (ctx->run_graph) cudaGraphExecDestroy(ctx->run_graph);

@@ -39,6 +39,7 @@
 // are 0.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "lya_internal.cuh"
 
@@ -67,7 +68,7 @@ struct DistParams {
   const double* __restrict__ odl2;
   const int32_t* __restrict__ f1;
   const int32_t* __restrict__ f2;
-  int64_t n_items;
+  const long long* n_items;   // [1] forest pairs of the queue (device: the captured graph serves any count)
   int max_len;
   double binner_rp, binner_rt;
   int np, nt, nb, cos_variant;
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
     if (tid == 0) s_item = (long long)atomicAdd(p.next, 1ull);
     __syncthreads();
     const long long t_item = s_item;
-    if (t_item >= p.n_items) break;
+    if (t_item >= *p.n_items) break;
     const int a = p.f1[t_item], b = p.f2[t_item];
     const int L1 = p.len[a], L2 = p.len[b];
     if (L1 <= 0 || L2 <= 0) { __syncthreads(); continue; }
@@ -454,48 +455,77 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   if (smem > 227 * 1024)
     return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory", max_len, smem);
   const int grid = ctx->num_sms;
-  double *d_D = nullptr, *d_W = nullptr, *col = nullptr, *moments = nullptr;
-  unsigned long long* err = nullptr;
-  cudaError_t e = lya_alloc(&d_D, (size_t)nb * nb);
-  if (e == cudaSuccess) e = lya_alloc(&d_W, nb);
-  if (e == cudaSuccess) e = lya_alloc(&col, (size_t)grid * 2 * 2 * max_len * TS * np);
-  if (e == cudaSuccess) e = lya_alloc(&moments, (size_t)grid * 4 * nt * np);
-  if (e == cudaSuccess) e = lya_alloc(&err, 2);
-  auto cleanup = [&]() { lya_free(d_D); lya_free(d_W); lya_free(col); lya_free(moments); lya_free(err); };
-  if (e != cudaSuccess) {
-    cleanup();
-    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_dist_run: device allocation failed");
+  // scratch and outputs kept in the context, so later calls (one per healpix
+  // pixel in the drop-in driver) allocate nothing and replay the captured graph
+  DistScratch& ds = ctx->dist;
+  if (!ds.D || ds.nb != nb || ds.max_len < max_len || ds.grid != grid) {
+    lya_free(ds.D); lya_free(ds.W); lya_free(ds.col); lya_free(ds.mom); lya_free(ds.err);
+    if (ds.graph) { cudaGraphExecDestroy(ds.graph); ds.graph = nullptr; }
+    ds = DistScratch{};
+    cudaError_t e = lya_alloc(&ds.D, (size_t)nb * nb);
+    if (e == cudaSuccess) e = lya_alloc(&ds.W, nb);
+    if (e == cudaSuccess) e = lya_alloc(&ds.col, (size_t)grid * 2 * 2 * max_len * TS * np);
+    if (e == cudaSuccess) e = lya_alloc(&ds.mom, (size_t)grid * 4 * nt * np);
+    if (e == cudaSuccess) e = lya_alloc(&ds.err, 3);
+    if (e != cudaSuccess) {
+      lya_free(ds.D); lya_free(ds.W); lya_free(ds.col); lya_free(ds.mom); lya_free(ds.err);
+      ds = DistScratch{};
+      return lya_fail(ctx, LYA_ERR_ALLOC, "lya_dist_run: device allocation failed");
+    }
+    ds.nb = nb; ds.max_len = max_len; ds.grid = grid;
   }
   cudaStream_t s = ctx->stream;
-  e = cudaMemsetAsync(d_D, 0, sizeof(double) * (size_t)nb * nb, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_W, 0, sizeof(double) * nb, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 2 * sizeof(unsigned long long), s);
-  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
-  if (e == cudaSuccess && ctx->wq.n_pairs > 0) {
-    DistParams p;
-    p.pix8 = ctx->cat.pix8; p.dl = ctx->cat.dl; p.pstart = ctx->cat.pstart; p.len = ctx->cat.len;
-    p.sorted = ctx->cat.sorted; p.ux = ctx->cat.ux; p.uy = ctx->cat.uy; p.uz = ctx->cat.uz;
-    p.omega = ctx->cat.omega; p.odl2 = ctx->cat.odl2; p.f1 = ctx->wq.f1; p.f2 = ctx->wq.f2;
-    p.n_items = ctx->wq.n_pairs; p.max_len = max_len;
-    p.binner_rp = (double)np / ctx->rpmax; p.binner_rt = (double)nt / ctx->rtmax;
-    p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant; p.npad = npad;
-    p.col = col; p.moments = moments; p.D = d_D; p.W = d_W; p.err = err; p.next = err + 1;
-    e = cudaFuncSetAttribute(k_dist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long n_items = ctx->wq.n_pairs;
+  DistParams p;
+  memset(&p, 0, sizeof(p));   // padding bytes take part in the graph key
+  p.pix8 = ctx->cat.pix8; p.dl = ctx->cat.dl; p.pstart = ctx->cat.pstart; p.len = ctx->cat.len;
+  p.sorted = ctx->cat.sorted; p.ux = ctx->cat.ux; p.uy = ctx->cat.uy; p.uz = ctx->cat.uz;
+  p.omega = ctx->cat.omega; p.odl2 = ctx->cat.odl2; p.f1 = ctx->wq.f1; p.f2 = ctx->wq.f2;
+  p.n_items = reinterpret_cast<const long long*>(ds.err + 2); p.max_len = ds.max_len;
+  p.binner_rp = (double)np / ctx->rpmax; p.binner_rt = (double)nt / ctx->rtmax;
+  p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant; p.npad = npad;
+  p.col = ds.col; p.moments = ds.mom; p.D = ds.D; p.W = ds.W; p.err = ds.err; p.next = ds.err + 1;
+  const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len) + sizeof(int) * (6 * (size_t)ds.max_len);
+  static_assert(sizeof(DistParams) <= sizeof(ds.key), "graph key does not fit");
+  cudaError_t e = cudaSuccess;
+  if (!ds.graph || memcmp(ds.key, &p, sizeof(p)) != 0) {
+    if (ds.graph) { cudaGraphExecDestroy(ds.graph); ds.graph = nullptr; }
+    e = cudaFuncSetAttribute(k_dist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_run);
+    cudaGraph_t g = nullptr;
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      k_dist<<<grid, DT, smem, s>>>(p);
-      ctx->launches++;
-      e = cudaGetLastError();
+      cudaError_t eq = cudaMemsetAsync(ds.D, 0, sizeof(double) * (size_t)nb * nb, s);
+      if (eq == cudaSuccess) eq = cudaMemsetAsync(ds.W, 0, sizeof(double) * nb, s);
+      if (eq == cudaSuccess) eq = cudaMemsetAsync(ds.err, 0, 2 * sizeof(unsigned long long), s);
+      if (eq == cudaSuccess) {
+        k_dist<<<grid, DT, smem_run, s>>>(p);
+        eq = cudaGetLastError();
+      }
+      const cudaError_t ec = cudaStreamEndCapture(s, &g);
+      e = eq != cudaSuccess ? eq : ec;
     }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ds.graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      ds.graph = nullptr;
+      return lya_fail(ctx, LYA_ERR_CUDA, "lya_dist_run: capture: %s", cudaGetErrorString(e));
+    }
+    memcpy(ds.key, &p, sizeof(p));
   }
-  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
+  e = cudaMemcpyAsync(ds.err + 2, &n_items, sizeof(n_items), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
+  if (e == cudaSuccess) e = cudaGraphLaunch(ds.graph, s);
+  if (e == cudaSuccess) {
+    ctx->launches++;
+    e = cudaEventRecord(ctx->ev1, s);
+  }
   unsigned long long nerr = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&nerr, err, sizeof(nerr), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && D) e = cudaMemcpyAsync(D, d_D, sizeof(double) * (size_t)nb * nb, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && W) e = cudaMemcpyAsync(W, d_W, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nerr, ds.err, sizeof(nerr), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && D) e = cudaMemcpyAsync(D, ds.D, sizeof(double) * (size_t)nb * nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && W) e = cudaMemcpyAsync(W, ds.W, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   float ms = 0.f;
   if (e == cudaSuccess) cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  cleanup();
   if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_dist_run: %s", cudaGetErrorString(e));
   ctx->last.kernel_ms = ms;
   if (nerr) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: %llu pixels pair into more than %d rt bins", nerr, TS);

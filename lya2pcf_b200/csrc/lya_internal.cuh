@@ -74,6 +74,18 @@ struct WorkQueue {
   double ref_pixels = 0.0;     // sum len1+len2
 };
 
+// Scratch, outputs and captured graph of lya_dist_run (kept between calls).
+struct DistScratch {
+  double* D = nullptr;                 // [nb][nb]
+  double* W = nullptr;                 // [nb]
+  double* col = nullptr;               // column scratch of every CTA
+  double* mom = nullptr;               // moment scratch of every CTA
+  unsigned long long* err = nullptr;   // [3]: span errors, work counter, item count
+  int nb = 0, max_len = 0, grid = 0;
+  cudaGraphExec_t graph = nullptr;     // clear + distortion kernel
+  alignas(16) unsigned char key[512] = {};   // the kernel parameters it was captured with
+};
+
 struct lya_ctx {
   int device = 0;
   int num_sms = 148;
@@ -119,6 +131,8 @@ struct lya_ctx {
   int64_t graph_launches = 0;            // runs replayed from the captured graph
 
   lya_stats_t last{};
+
+  DistScratch dist;
 
   // covariance post-processing: the last covariance, kept for lya_covariance_smooth
   double* cov = nullptr;                 // [cov_nb][cov_nb]
