@@ -102,6 +102,26 @@ int lya_upload_forests(lya_ctx* ctx, int64_t n_forests, const int64_t* start, co
                        const double* uz, const double* ra, const double* dec, const int64_t* name,
                        const int32_t* owner_slot, int32_t n_slots, const double* omega, const double* odl2);
 
+/* Catalogue upload from the deltas, with the projection done on the device:
+ * replaces the per-quasar fill_dw(delta, loglam, project) of the ingest
+ * (delta_reader.py:53, forest_class.py:48-68).  Arguments as
+ * lya_upload_forests, with delta (per pixel) in place of dw and
+ * log10(lambda) (loglam, per pixel) in place of dl; dw, the deltas' weighted
+ * log-lambda offsets dl, omega = sum w and odl2 = sum w dl^2 are computed per
+ * forest on the device (project = 1), or dw = delta w with dl, omega, odl2 = 0
+ * (project = 0), exactly as fill_dw.  A forest whose weights sum to 0 is
+ * LYA_ERR_DATA (numpy's average raises there). */
+int lya_upload_deltas(lya_ctx* ctx, int64_t n_forests, const int64_t* start, const double* dc, const double* w,
+                      const double* delta, const double* z, const double* loglam, const double* ux, const double* uy,
+                      const double* uz, const double* ra, const double* dec, const int64_t* name,
+                      const int32_t* owner_slot, int32_t n_slots, int32_t project);
+
+/* The catalogue's dw, dl (per pixel, CSR order) and omega, odl2 (per forest)
+ * as uploaded or as projected by lya_upload_deltas (host arrays; any may be
+ * NULL).  The quasar attributes dw, delta_lambda, omega, omega_delta_lambda2
+ * of forest_class.py:42-46. */
+int lya_get_projection(lya_ctx* ctx, double* dw, double* dl, double* omega, double* odl2);
+
 /* Neighbour lists on the device; replaces quasar.neighborhood
  * (forest_class.py:78-98) called per forest by two_point_per_pixel
  * (correlation_procedures_pycuda.py:144): f2 is a neighbour of f1 when

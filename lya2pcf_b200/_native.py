@@ -31,6 +31,8 @@ SIGNATURES = {
     'lya_version': ([], C.c_int),
     'lya_set_bins': ([P, C.c_double, C.c_double, C.c_int32, C.c_int32], C.c_int),
     'lya_upload_forests': ([P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32, P, P], C.c_int),
+    'lya_upload_deltas': ([P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32, C.c_int32], C.c_int),
+    'lya_get_projection': ([P, P, P, P, P], C.c_int),
     'lya_build_pairs': ([P, C.c_double, C.c_double, C.POINTER(C.c_int64)], C.c_int),
     'lya_set_pairs': ([P, C.c_int64, P, P], C.c_int),
     'lya_get_pairs': ([P, P, P], C.c_int),

@@ -171,11 +171,73 @@ __global__ void k_pack(int64_t n, const int64_t* __restrict__ start, const int64
   }
 }
 
-extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start, const double* dc, const double* w,
-                                  const double* dw, const double* z, const double* dl, const double* ux,
-                                  const double* uy, const double* uz, const double* ra, const double* dec,
-                                  const int64_t* name, const int32_t* owner_slot, int32_t n_slots,
-                                  const double* omega, const double* odl2) {
+// Device projection of the deltas, quasar.fill_dw (forest_class.py:48-68), one
+// block per forest: on entry dw holds delta and dl holds log10(lambda); on exit
+// dw = w (delta - <delta> - dl <dl delta>/<dl^2>), dl = loglam - <loglam>, and
+// omega = sum w, odl2 = sum dl^2 w (<.> weighted by w, in the reference's
+// operation order; <dl^2> = 0, e.g. a one-pixel forest, gives NaN as numpy
+// does).  project = 0: dw = delta w, dl = omega = odl2 = 0.  A forest whose
+// weights sum to 0 is counted in zero_w (numpy's average raises there).
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int k = 0; k < nw; ++k) t += red[k];
+  return t;
+}
+
+__global__ void k_project(int64_t n, const int64_t* __restrict__ start, const double* __restrict__ w,
+                          double* __restrict__ dw, double* __restrict__ dl, double* __restrict__ omega,
+                          double* __restrict__ odl2, int project, unsigned long long* __restrict__ zero_w) {
+  __shared__ double red[32];
+  for (int64_t f = blockIdx.x; f < n; f += gridDim.x) {
+    const int64_t a = start[f], L = start[f + 1] - a;
+    if (!project) {
+      for (int64_t k = threadIdx.x; k < L; k += blockDim.x) { dw[a + k] = dw[a + k] * w[a + k]; dl[a + k] = 0.0; }
+      if (threadIdx.x == 0) { omega[f] = 0.0; odl2[f] = 0.0; }
+      continue;
+    }
+    double sw = 0.0, swd = 0.0, swl = 0.0;
+    for (int64_t k = threadIdx.x; k < L; k += blockDim.x) {
+      const double wk = w[a + k];
+      sw += wk;
+      swd += dw[a + k] * wk;
+      swl += dl[a + k] * wk;
+    }
+    sw = block_sum(sw, red);
+    swd = block_sum(swd, red);
+    swl = block_sum(swl, red);
+    if (L > 0 && sw == 0.0 && threadIdx.x == 0) atomicAdd(zero_w, 1ull);
+    const double deltaprom = swd / sw, lam = swl / sw;
+    double s2 = 0.0, sld = 0.0;
+    for (int64_t k = threadIdx.x; k < L; k += blockDim.x) {
+      const double wk = w[a + k], x = dl[a + k] - lam;
+      s2 += x * x * wk;
+      sld += x * dw[a + k] * wk;
+    }
+    s2 = block_sum(s2, red);
+    sld = block_sum(sld, red);
+    const double ldprom = sld / sw, llprom = s2 / sw;
+    for (int64_t k = threadIdx.x; k < L; k += blockDim.x) {
+      const double wk = w[a + k], x = dl[a + k] - lam;
+      dw[a + k] = wk * ((dw[a + k] - deltaprom) - x * ldprom / llprom);
+      dl[a + k] = x;
+    }
+    if (threadIdx.x == 0) { omega[f] = sw; odl2[f] = s2; }
+    __syncthreads();
+  }
+}
+
+// ingest: -1 = forests with dw, dl, omega, odl2 given; 0 or 1 = deltas and
+// log-lambda given in dw and dl, projected on the device (1) or not (0).
+static int upload_impl(lya_ctx* ctx, int64_t n, const int64_t* start, const double* dc, const double* w,
+                       const double* dw, const double* z, const double* dl, const double* ux, const double* uy,
+                       const double* uz, const double* ra, const double* dec, const int64_t* name,
+                       const int32_t* owner_slot, int32_t n_slots, const double* omega, const double* odl2,
+                       int ingest) {
   if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_upload_forests: ctx is NULL");
   if (n < 0 || n >= (int64_t)INT32_MAX) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: bad n_forests %lld",
                                                        (long long)n);
@@ -215,7 +277,7 @@ extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start,
   DevCatalog& c = ctx->cat;
   c.n = n; c.npix = npix; c.npad = npad; c.n_slots = n_slots;
   c.has_dl = dl != nullptr;
-  c.has_moments = omega != nullptr && odl2 != nullptr;
+  c.has_moments = (omega != nullptr && odl2 != nullptr) || ingest >= 0;
 
   cudaError_t e = cudaSuccess;
 #define ALLOC(p, cnt) if (e == cudaSuccess) e = lya_alloc(&(p), (size_t)(cnt))
@@ -260,6 +322,17 @@ extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start,
   if (e == cudaSuccess) e = cudaMemsetAsync(c.pix8, 0, sizeof(double4) * npad, s);
   if (e == cudaSuccess && !omega) e = cudaMemsetAsync(c.omega, 0, sizeof(double) * n, s);
   if (e == cudaSuccess && !odl2) e = cudaMemsetAsync(c.odl2, 0, sizeof(double) * n, s);
+  unsigned long long* zero_w = nullptr;
+  if (e == cudaSuccess && ingest >= 0 && n > 0) {
+    e = lya_alloc(&zero_w, 1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(zero_w, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) {
+      const int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
+      k_project<<<blocks, 128, 0, s>>>(n, t_start, t_w, t_dw, t_dl, c.omega, c.odl2, ingest, zero_w);
+      ctx->launches++;
+      e = cudaGetLastError();
+    }
+  }
   if (e == cudaSuccess && n > 0) {
     int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
     k_pack<<<blocks, 128, 0, s>>>(n, t_start, c.pstart, t_dc, t_w, t_dw, t_z, t_dl, c.dc, c.w, c.dw, c.z, c.dl,
@@ -269,15 +342,65 @@ extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start,
   }
   // forests the FP32 kernel's lean walk cannot take (they need the second pass)
   std::vector<uint8_t> flags((size_t)n);
+  unsigned long long nzero = 0;
   if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(flags.data(), c.sorted, (size_t)n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && zero_w) e = cudaMemcpyAsync(&nzero, zero_w, sizeof(nzero), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  lya_free(zero_w);
   cleanup_tmp();
+  if (e == cudaSuccess && nzero) {
+    lya_free_catalog(ctx->cat);
+    return lya_fail(ctx, LYA_ERR_DATA, "lya_upload_deltas: %llu forests have weights summing to 0", nzero);
+  }
   if (e != cudaSuccess) {
     lya_free_catalog(ctx->cat);
     return lya_fail(ctx, LYA_ERR_CUDA, "lya_upload_forests: %s", cudaGetErrorString(e));
   }
   c.n_not_lean = 0;
   for (int64_t f = 0; f < n; ++f) c.n_not_lean += (flags[f] & LYA_LEAN) ? 0 : 1;
+  return LYA_OK;
+}
+
+extern "C" int lya_upload_forests(lya_ctx* ctx, int64_t n, const int64_t* start, const double* dc, const double* w,
+                                  const double* dw, const double* z, const double* dl, const double* ux,
+                                  const double* uy, const double* uz, const double* ra, const double* dec,
+                                  const int64_t* name, const int32_t* owner_slot, int32_t n_slots,
+                                  const double* omega, const double* odl2) {
+  return upload_impl(ctx, n, start, dc, w, dw, z, dl, ux, uy, uz, ra, dec, name, owner_slot, n_slots, omega, odl2,
+                     -1);
+}
+
+extern "C" int lya_upload_deltas(lya_ctx* ctx, int64_t n, const int64_t* start, const double* dc, const double* w,
+                                 const double* delta, const double* z, const double* loglam, const double* ux,
+                                 const double* uy, const double* uz, const double* ra, const double* dec,
+                                 const int64_t* name, const int32_t* owner_slot, int32_t n_slots, int32_t project) {
+  if (ctx && start && n > 0 && start[n] > 0 && !loglam)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_deltas: loglam is NULL");
+  return upload_impl(ctx, n, start, dc, w, delta, z, loglam, ux, uy, uz, ra, dec, name, owner_slot, n_slots, nullptr,
+                     nullptr, project ? 1 : 0);
+}
+
+extern "C" int lya_get_projection(lya_ctx* ctx, double* dw, double* dl, double* omega, double* odl2) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_get_projection: ctx is NULL");
+  const DevCatalog& c = ctx->cat;
+  if (c.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_get_projection: no forests uploaded");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  std::vector<double> pad((size_t)c.npad);
+  for (int k = 0; k < 2; ++k) {
+    double* out = k == 0 ? dw : dl;
+    if (!out) continue;
+    LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(pad.data(), k == 0 ? c.dw : c.dl, sizeof(double) * c.npad,
+                                        cudaMemcpyDeviceToHost, s));
+    LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    for (int64_t f = 0; f < c.n; ++f) {
+      const int64_t a = ctx->h_start[f], L = ctx->h_start[f + 1] - a;
+      std::copy(pad.begin() + ctx->h_pstart[f], pad.begin() + ctx->h_pstart[f] + L, out + a);
+    }
+  }
+  if (omega) LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(omega, c.omega, sizeof(double) * c.n, cudaMemcpyDeviceToHost, s));
+  if (odl2) LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(odl2, c.odl2, sizeof(double) * c.n, cudaMemcpyDeviceToHost, s));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   return LYA_OK;
 }
 

@@ -87,6 +87,36 @@ class PairEngine:
         self.n_pairs = 0
         return self
 
+    def upload_deltas(self, fs, delta, loglam, project=True):
+        """Upload the geometry and weights of ``fs`` with per-pixel ``delta`` and
+        log10(lambda) ``loglam``; the projection of ``quasar.fill_dw``
+        (``forest_class.py:48-68``) runs on the device.  ``fs.dw``, ``fs.dl``,
+        ``fs.omega`` and ``fs.odl2`` are not read; :meth:`projection` returns
+        the device's."""
+        slot, slot_pixels = owner_slots(fs.pix)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        arrs = dict(start=np.ascontiguousarray(fs.start, dtype=np.int64), dc=f64(fs.dc), w=f64(fs.w),
+                    delta=f64(delta), z=f64(fs.z), loglam=f64(loglam), ux=f64(fs.ux), uy=f64(fs.uy), uz=f64(fs.uz),
+                    ra=f64(fs.ra), dec=f64(fs.dec), name=np.ascontiguousarray(fs.name, dtype=np.int64),
+                    slot=np.ascontiguousarray(slot, dtype=np.int32))
+        p = N.ptr
+        self._check(self.lib.lya_upload_deltas(
+            self.ctx, fs.n, p(arrs['start']), p(arrs['dc']), p(arrs['w']), p(arrs['delta']), p(arrs['z']),
+            p(arrs['loglam']), p(arrs['ux']), p(arrs['uy']), p(arrs['uz']), p(arrs['ra']), p(arrs['dec']),
+            p(arrs['name']), p(arrs['slot']), int(len(slot_pixels)), 1 if project else 0))
+        self.fs = fs
+        self.slot_of_forest = slot
+        self.slot_pixels = slot_pixels
+        self.n_pairs = 0
+        return self
+
+    def projection(self):
+        """``(dw[npix], dl[npix], omega[n], odl2[n])`` of the uploaded catalogue."""
+        n, npix = self.fs.n, self.fs.npix_total
+        dw, dl, om, o2 = np.zeros(npix), np.zeros(npix), np.zeros(n), np.zeros(n)
+        self._check(self.lib.lya_get_projection(self.ctx, N.ptr(dw), N.ptr(dl), N.ptr(om), N.ptr(o2)))
+        return dw, dl, om, o2
+
     # ------------------------------------------------------------------ work queue
     def build_pairs(self, angmax):
         """Neighbour search on the device (``quasar.neighborhood`` for every forest)."""

@@ -71,6 +71,24 @@ class ForestSet:
             groups.setdefault(p, []).append(f)
         return groups
 
+    # ------------------------------------------------------------------ columnar cache
+    _COLUMNS = ('start', 'dc', 'w', 'dw', 'z', 'dl', 'ra', 'dec', 'ux', 'uy', 'uz', 'name', 'pix', 'omega', 'odl2')
+
+    def save(self, path):
+        """Write the catalogue as one ``.npz`` of columns: a cache that later
+        runs load in place of unpickling ``data#.npy`` quasar objects."""
+        np.savez(path, **{k: getattr(self, k) for k in self._COLUMNS},
+                 meta_keys=np.array(list(self.meta.keys()), dtype=object),
+                 meta_values=np.array([str(v) for v in self.meta.values()], dtype=object))
+
+    @classmethod
+    def load(cls, path):
+        """Read a catalogue written by :meth:`save`."""
+        with np.load(path, allow_pickle=True) as z:
+            cols = {k: z[k] for k in cls._COLUMNS}
+            meta = dict(zip(z['meta_keys'].tolist(), z['meta_values'].tolist())) if 'meta_keys' in z else {}
+        return cls(meta=meta, **cols)
+
     # ------------------------------------------------------------------ dict form
     def to_quasar_dict(self):
         """The reference's ``data`` object: dict pixel -> list of ``forest_class.quasar``."""
