@@ -11,7 +11,8 @@ unchanged.  With ``--gpu`` it also writes ``corr_dir/pairs_2d_pixel_<pixel>.npz`
 (pair counts, weighted mean r_par / r_perp / z), whose names do not match the
 ``2d_histogram_pixel_*`` glob of ``post_processing.py``.
 
-Ranks: mpi4py when installed (as the reference), else a single process.  The
+Ranks: mpi4py when installed (as the reference), else torchrun's torch.distributed
+environment, else a single process (lya2pcf_b200.ranks).  The
 GPU of a rank is ``rank % number_of_cuda_devices + cuda_device_first_number``
 (``2pla.py:21``).  Pixels are split into contiguous runs balanced by pair
 count instead of ``np.array_split`` by pixel count.
@@ -29,19 +30,14 @@ sys.path.insert(1, os.path.dirname(os.path.dirname(_here)))
 from parameters import *   # noqa: E402,F401,F403
 import parameters as _P   # noqa: E402
 from forest_class import quasar   # noqa: E402,F401  (unpickling needs it)
+from lya2pcf_b200.ranks import Ranks   # noqa: E402
 
 
-def _comm():
-    try:
-        from mpi4py import MPI
-        c = MPI.COMM_WORLD
-        return c, c.Get_rank(), c.Get_size()
-    except ImportError:
-        return None, 0, 1
 
 
 def main():
-    comm, rank, size = _comm()
+    ranks = Ranks()
+    rank, size = ranks.rank, ranks.size
     os.environ['CUDA_DEVICE'] = str(int(rank % _P.number_of_cuda_devices + _P.cuda_device_first_number))
     parser = argparse.ArgumentParser(description='Takes the data.npy file and computes the two point correlation '
                                                  'function histograms.')
@@ -93,6 +89,7 @@ def main():
             print('Exiting early due to --verbose option.')
             break
     log_file.close()
+    ranks.close()
     print('Finished correlation computation.')
 
 

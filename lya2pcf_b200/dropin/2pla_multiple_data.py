@@ -32,15 +32,9 @@ sys.path.insert(1, os.path.dirname(os.path.dirname(_here)))
 from parameters import *   # noqa: E402,F401,F403
 import parameters as _P   # noqa: E402
 from forest_class import quasar   # noqa: E402,F401  (unpickling needs it)
+from lya2pcf_b200.ranks import Ranks   # noqa: E402
 
 
-def _comm():
-    try:
-        from mpi4py import MPI
-        c = MPI.COMM_WORLD
-        return c, c.Get_rank(), c.Get_size()
-    except ImportError:
-        return None, 0, 1
 
 
 def _angmax(data):
@@ -62,7 +56,8 @@ def _bin_file(correlations, data, corr_dir, log_file, gpu, pixels, verbose):
 
 
 def main(argv=None):
-    comm, rank, size = _comm()
+    ranks = Ranks()
+    rank, size = ranks.rank, ranks.size
     os.environ['CUDA_DEVICE'] = str(int(rank % _P.number_of_cuda_devices + _P.cuda_device_first_number))
     parser = argparse.ArgumentParser(description='Computes the two point correlation histograms of every data*.npy '
                                                  'file of a directory.')
@@ -100,6 +95,7 @@ def main(argv=None):
         mine = [p for p in np.array_split(np.array(pixels, dtype=object), size)[rank]]
         _bin_file(correlations, data, corr_dir, log_file, args.gpu, mine, args.verbose)
     log_file.close()
+    ranks.close()
     print('Finished correlation computation.')
     return 0
 

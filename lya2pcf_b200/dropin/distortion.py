@@ -5,7 +5,8 @@
 Loads ``data_dir/data1.npy``, computes angmax from the smallest first-pixel
 distance, sums ``distortion_per_pixel`` over this rank's pixels
 (``distortion.py:101-108``), adds the ranks' sums (mpi4py ``reduce`` when
-installed, as the reference at ``:118-119``) and saves
+installed, as the reference at ``:118-119``, else one torch.distributed
+reduce when started by torchrun) and saves
 ``corr_dir/distortion.npy = D / W[:, None]`` (``:125``).
 """
 import argparse
@@ -22,19 +23,12 @@ from parameters import *   # noqa: E402,F401,F403
 import parameters as _P   # noqa: E402
 from forest_class import quasar   # noqa: E402,F401  (unpickling needs it)
 import distortion_procedures_pycuda as distortion   # noqa: E402
-
-
-def _comm():
-    try:
-        from mpi4py import MPI
-        c = MPI.COMM_WORLD
-        return c, c.Get_rank(), c.Get_size()
-    except ImportError:
-        return None, 0, 1
+from lya2pcf_b200.ranks import Ranks   # noqa: E402
 
 
 def main():
-    comm, rank, size = _comm()
+    ranks = Ranks()
+    rank, size = ranks.rank, ranks.size
     os.environ['CUDA_DEVICE'] = str(int(rank % _P.number_of_cuda_devices + _P.cuda_device_first_number))
     parser = argparse.ArgumentParser(description='Takes the data.npy file and computes the distortion matrix of the '
                                                  'two point correlation function.')
@@ -65,12 +59,11 @@ def main():
         if args.verbose and count + 1 > 1:
             print('Exiting early due to --verbose option.')
             break
-    if size > 1:
-        disto = comm.reduce(disto)
-        weight_A = comm.reduce(weight_A)
+    disto, weight_A = ranks.reduce_sum(disto, weight_A)
     if rank == 0:
         with np.errstate(divide='ignore', invalid='ignore'):
             np.save(corr_dir + 'distortion', disto / weight_A[:, None])
+    ranks.close()
     print('Finished distortion computation.')
 
 

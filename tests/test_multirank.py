@@ -63,3 +63,37 @@ def test_two_gloo_ranks_cover_every_pixel_once():
     ok, mine, total = q.get(timeout=60)
     assert ok
     assert 0.3 * total < mine < 0.7 * total
+
+
+def _reduce_worker(rank, world, port, q):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    from lya2pcf_b200.ranks import Ranks
+    r = Ranks()
+    try:
+        rng = np.random.default_rng(rank)
+        d, w = rng.normal(size=(50, 50)), rng.uniform(size=50)
+        sd, sw = r.reduce_sum(d, w)
+        if r.rank == 0:
+            r1 = np.random.default_rng(1)
+            d1 = r1.normal(size=(50, 50))
+            w1 = r1.uniform(size=50)
+            q.put((bool(np.allclose(sd, d + d1, rtol=0, atol=1e-14)), bool(np.allclose(sw, w + w1, rtol=0, atol=1e-14)),
+                   r.size))
+    finally:
+        r.close()
+
+
+def test_distortion_reduction_over_torch_ranks():
+    """The drivers' rank helper without mpi4py: two torchrun-style gloo ranks;
+    rank 0 receives the sum of the ranks' distortion numerators and weights
+    (the single collective of the distortion driver)."""
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    mp.start_processes(_reduce_worker, args=(2, port, q), nprocs=2, join=True, start_method='spawn')
+    okd, okw, size = q.get(timeout=60)
+    assert okd and okw and size == 2
