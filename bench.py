@@ -427,17 +427,29 @@ def fp64_comparison(eng, fs, kern):
     rngs = (s0, min(nslot, s0 + 40))
     res = {}
     counts = {}
+    hists = {}
     for name, code in (('fp32_guarded', 0), ('fp64_diagonal', 1), ('fp64_plain', 2)):
         st = eng.run(kernel=code, guard=GUARD, slots=rngs)
         st = eng.run(kernel=code, guard=GUARD, slots=rngs)
         h, c = eng.histograms(rngs[0], rngs[1] - rngs[0])
         counts[name] = c
+        hists[name] = h
         res[name] = {'pairs_per_s': st['run_ref_pairs'] / (st['kernel_ms'] * 1e-3), 'kernel_ms': st['kernel_ms'],
                      'W_sum': float(h[:, 0].sum())}
     res['slots'] = list(rngs)
     res['ref_pairs'] = st['run_ref_pairs']
     res['counts_equal_fp32_fp64diag'] = bool(np.array_equal(counts['fp32_guarded'], counts['fp64_diagonal']))
     res['counts_equal_fp32_fp64plain'] = bool(np.array_equal(counts['fp32_guarded'], counts['fp64_plain']))
+    # accuracy of the FP32-guarded sums against the FP64 kernel (equal to the oracle to 1e-12 in the tests)
+    h32, h64 = hists['fp32_guarded'], hists['fp64_plain']
+    W32, W64 = h32[:, 0], h64[:, 0]
+    nz = W64 > 0
+    xi32 = np.divide(h32[:, 1], W32, out=np.zeros_like(W32), where=W32 != 0)
+    xi64 = np.divide(h64[:, 1], W64, out=np.zeros_like(W64), where=W64 != 0)
+    res['max_rel_err_W'] = float(np.max(np.abs(W32 - W64)[nz] / W64[nz])) if nz.any() else 0.0
+    res['max_rel_err_RP_RT_Z'] = [float(np.max(np.abs(h32[:, q] - h64[:, q])[nz] / np.abs(h64[:, q])[nz]))
+                                  for q in (2, 3, 4)] if nz.any() else None
+    res['max_err_xi_over_max_xi'] = float(np.abs(xi32 - xi64).max() / max(np.abs(xi64).max(), 1e-300))
     res['speedup_fp32_vs_fp64plain'] = res['fp32_guarded']['pairs_per_s'] / res['fp64_plain']['pairs_per_s']
     res['speedup_fp32_vs_fp64diag'] = res['fp32_guarded']['pairs_per_s'] / res['fp64_diagonal']['pairs_per_s']
     return res
