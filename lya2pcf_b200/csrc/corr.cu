@@ -856,8 +856,11 @@ struct LeanWalk {
     }
   }
 
-  // One step with event handling: pair a = (q1, qa), pair b = (q1, qb).
-  __device__ __forceinline__ void slow_step(int k, const float4& q1, float z1, const float4& qa, float za,
+  // One step: pair a = (q1, qa), pair b = (q1, qb), with the warp's events.
+  // There is no event-free fast path: with 64 diagonals per warp and runs of
+  // about 30 pairs, some lane leaves its run on almost every step, so a
+  // warp-wide "no event" test before the step costs more than it saves.
+  __device__ __forceinline__ void step(int k, const float4& q1, float z1, const float4& qa, float za,
                                             const float4& qb, float zb) {
     const float ea = lean_e(q1, qa), sa = lean_s(q1, qa);
     const float eb = lean_e(q1, qb), sb = lean_s(q1, qb);
@@ -972,23 +975,8 @@ __device__ void item_lean(const CorrParams& p, int64_t t, const SmemHist& h, Rec
     for (; k < W.kall; k += 2) {
       const float4 q1b = A1[k + 1], q2z = A2[k + 2];
       const float z1b = Z1[k + 1], z2z = Z2[k + 2];
-      const float e0a = lean_e(q1a, q2x), s0a = lean_s(q1a, q2x);
-      const float e0b = lean_e(q1a, q2y), s0b = lean_s(q1a, q2y);
-      const float e1a = lean_e(q1b, q2y), s1a = lean_s(q1b, q2y);
-      const float e1b = lean_e(q1b, q2z), s1b = lean_s(q1b, q2z);
-      const bool a0 = k >= W.ka_beg && k < W.ka_end, b0 = k >= W.kb_beg && k < W.kb_end;
-      const bool a1 = k + 1 >= W.ka_beg && k + 1 < W.ka_end, b1 = k + 1 >= W.kb_beg && k + 1 < W.kb_end;
-      const bool ev = (a0 && lean_out(W.ra, e0a, s0a)) || (b0 && lean_out(W.rb, e0b, s0b)) ||
-                      (a1 && lean_out(W.ra, e1a, s1a)) || (b1 && lean_out(W.rb, e1b, s1b));
-      if (__any_sync(FULL, ev)) {
-        W.slow_step(k, q1a, z1a, q2x, z2x, q2y, z2y);
-        W.slow_step(k + 1, q1b, z1b, q2y, z2y, q2z, z2z);
-      } else {
-        if (a0) W.acca.add(q1a, z1a, q2x, z2x, e0a, s0a);
-        if (b0) W.accb.add(q1a, z1a, q2y, z2y, e0b, s0b);
-        if (a1) W.acca.add(q1b, z1b, q2y, z2y, e1a, s1a);
-        if (b1) W.accb.add(q1b, z1b, q2z, z2z, e1b, s1b);
-      }
+      W.step(k, q1a, z1a, q2x, z2x, q2y, z2y);
+      W.step(k + 1, q1b, z1b, q2y, z2y, q2z, z2z);
       q1a = A1[k + 2];
       z1a = Z1[k + 2];
       q2x = q2z;
