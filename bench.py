@@ -467,8 +467,10 @@ def dram_traffic_per_launch(ref_pairs):
 
 def alu_roofline(st, kms, clk):
     """Pair evaluations per second against the FP32 issue bound: the FP32
-    operations one pixel pair needs (the reference's 10 + 7 for the new
-    outputs, SURVEY cost model) at the B200's FP32 rate."""
+    operations one pixel pair needs (10 in the reference kernel,
+    cuda_kernels.cpp:142-155: rp sub+mul, rt add+mul, two bin scalings, two
+    weight products, two accumulations; 7 more for the count-free new outputs:
+    three products and four accumulations) at the B200's FP32 rate."""
     evals = st['evaluated_pairs'] / (kms * 1e-3)
     sm_mhz = (clk or {}).get('sm_mhz') or 1965.0
     fp32_lanes = 148 * 128 * sm_mhz * 1e6        # FP32 lane-instructions per second
