@@ -5,7 +5,8 @@ Runs in a container where the lya2pcf reference tree is mounted (default
 reference's numba CPU kernel ``correlation_procedures_cpu.pair_correlation``
 (``correlation_procedures_cpu.py:46-84``) and its ``two_point_per_pixel`` driver
 (``:19-43``), feeds them seeded synthetic forests, and stores inputs and outputs
-as ``.npz``.  The GPU test machine has no reference tree; it only reads the
+as ``.npz`` (``numba_pairs``: hand-placed pairs; ``numba_sweep``: seeded random
+pairs over the whole sky; ``numba_pixel``: one pixel through the driver).  The GPU test machine has no reference tree; it only reads the
 committed ``.npz`` files.
 
     python tests/golden/make_golden.py
@@ -108,6 +109,48 @@ def main():
     del order
     np.savez_compressed(os.path.join(OUT, 'numba_pixel.npz'), **payload)
     print('wrote numba_pixel.npz')
+    sweep(cpu, refpar, angmax)
+
+
+def _offset(ra1, dec1, sep, pa):
+    """The point at angular distance sep and position angle pa from (ra1, dec1)."""
+    dec2 = np.arcsin(np.sin(dec1) * np.cos(sep) + np.cos(dec1) * np.sin(sep) * np.cos(pa))
+    ra2 = ra1 + np.arctan2(np.sin(pa) * np.sin(sep) * np.cos(dec1), np.cos(sep) - np.sin(dec1) * np.sin(dec2))
+    return float(np.mod(ra2, 2 * np.pi)), float(dec2)
+
+
+def sweep(cpu, refpar, angmax, n_cases=32):
+    """numba_sweep.npz: seeded random forest pairs over the whole sky through
+    the reference numba pair_correlation, same layout as numba_pairs.npz.
+    Declinations up to +-80 deg, a quarter of the pairs straddling ra = 0 / 2 pi,
+    separations up to 1.05 angmax (the reference's angle cut, ``:69``, drops
+    the farthest), lengths 1..250 anywhere on the 614-pixel grid."""
+    rng = np.random.default_rng(11)
+    deg = np.pi / 180
+    cases = []
+    for c in range(n_cases):
+        dec1 = rng.uniform(-80.0, 80.0) * deg
+        ra1 = rng.uniform(0.0, 2 * np.pi) if c % 4 else float(np.mod(rng.uniform(-0.5, 0.5) * deg, 2 * np.pi))
+        sep = angmax * rng.uniform(0.0, 1.05)
+        ra2, dec2 = _offset(ra1, dec1, sep, rng.uniform(0.0, 2 * np.pi))
+        l1, l2 = (int(x) for x in rng.integers(1, 251, 2))
+        s1, s2 = (int(x) for x in rng.integers(0, 614 - 250, 2))
+        a = _forest(rng, l1, s1, ra1, dec1)
+        b = _forest(rng, l2, s2, ra2, dec2)
+        wh, dwh = cpu.pair_correlation(angmax, a['ra'], a['dec'], a['w'], a['dw'], 0, a['dc'], 0,
+                                       b['ra'], b['dec'], b['w'], b['dw'], 0, b['dc'], 0)
+        cases.append((a, b, wh, dwh))
+    payload = {'angmax': angmax, 'n_cases': len(cases), 'rpmax': float(refpar.rpmax), 'rtmax': float(refpar.rtmax),
+               'np': int(refpar.numpix_rp), 'nt': int(refpar.numpix_rt)}
+    for c, (a, b, wh, dwh) in enumerate(cases):
+        for tag, f in (('a', a), ('b', b)):
+            for k, v in f.items():
+                payload[f'c{c}_{tag}_{k}'] = np.asarray(v)
+        payload[f'c{c}_w_hist'] = wh
+        payload[f'c{c}_dw_hist'] = dwh
+    np.savez_compressed(os.path.join(OUT, 'numba_sweep.npz'), **payload)
+    nonzero = sum(int(np.count_nonzero(wh) > 0) for _, _, wh, _ in cases)
+    print('wrote numba_sweep.npz with', len(cases), 'forest pairs,', nonzero, 'with pairs in range')
 
 
 if __name__ == '__main__':

@@ -7,6 +7,7 @@ from oracle import oracle as O
 
 G_PAIRS = 'tests/golden/numba_pairs.npz'
 G_PIXEL = 'tests/golden/numba_pixel.npz'
+G_SWEEP = 'tests/golden/numba_sweep.npz'
 
 
 def _load(name):
@@ -21,9 +22,12 @@ def _pair_fs(g, c):
     return forestset([fa, fb])
 
 
-def test_numba_pairs_bit_exact():
-    """CPU-formula oracle == the reference numba pair_correlation, bit for bit."""
-    g = _load(G_PAIRS)
+@pytest.mark.parametrize('golden', [G_PAIRS, G_SWEEP])
+def test_numba_pairs_bit_exact(golden):
+    """CPU-formula oracle == the reference numba pair_correlation, bit for bit
+    (hand-placed pairs, and a seeded whole-sky sweep: high declinations, the
+    ra = 0 / 2 pi wrap, separations around the angle cut)."""
+    g = _load(golden)
     for c in range(int(g['n_cases'])):
         fs = _pair_fs(g, c)
         out, cnt = O.corr(fs, [0], [1], [0, 1], mode=O.CPU_FORMULA, angmax=float(g['angmax']))
@@ -46,11 +50,20 @@ def test_numba_pixel_bit_exact():
     assert np.array_equal(out[0, O.Q_DW].reshape(50, 50), g['dw_hist'])
 
 
-def test_gpu_formula_agrees_with_cpu_formula_on_golden_cases():
+@pytest.mark.parametrize('golden', [G_PAIRS, G_SWEEP])
+def test_gpu_formula_agrees_with_cpu_formula_on_golden_cases(golden):
     """The two reference formulas differ only near bin edges; on the golden
-    cases they give the same bins and sums within rounding."""
-    g = _load(G_PAIRS)
+    cases they give the same bins and sums within rounding.  The GPU kernel has
+    no angle cut (the neighbour search applies it), so sweep pairs at or beyond
+    angmax are left out."""
+    g = _load(golden)
+    angmax = float(g['angmax'])
     for c in range(int(g['n_cases'])):
+        ra1, dec1, ra2, dec2 = (float(g[f'c{c}_{t}_{k}']) for t, k in (('a', 'ra'), ('a', 'dec'), ('b', 'ra'),
+                                                                       ('b', 'dec')))
+        cosang = np.sin(dec1) * np.sin(dec2) + np.cos(dec1) * np.cos(dec2) * np.cos(ra1 - ra2)
+        if not np.arccos(min(1.0, cosang)) < angmax * (1 - 1e-9):
+            continue
         fs = _pair_fs(g, c)
         oc, cc = O.corr(fs, [0], [1], [0, 1], mode=O.CPU_FORMULA, angmax=float(g['angmax']))
         og, cg = O.corr(fs, [0], [1], [0, 1], mode=O.GPU_FORMULA)
