@@ -109,6 +109,31 @@ def test_edge_catalog(kern, var):
 
 
 @pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
+def test_whole_sky_sweep_pairs(kern, var):
+    """The seeded whole-sky golden sweep (high declinations, pairs across
+    ra = 0 / 2 pi; its CPU-formula histograms pin the oracle to the reference
+    numba kernel): one owner slot per forest pair, counts bit-exact against the
+    oracle's GPU formula, sums within the kernel's tolerance."""
+    import os
+    from helpers import forestset
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'numba_sweep.npz'))
+    keys = ('ra', 'dec', 'dc', 'w', 'dw', 'z')
+    n = int(g['n_cases'])
+    fs = forestset([{k: g[f'c{c}_{t}_{k}'] for k in keys} for c in range(n) for t in ('a', 'b')],
+                   pix=np.repeat(np.arange(n), 2))
+    f1 = np.arange(0, 2 * n, 2, dtype=np.int32)
+    f2 = f1 + 1
+    ho, co = O.corr(fs, f1, f2, np.arange(n + 1))
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.set_pairs(f1, f2)
+        eng.run(kernel=kern, variant=var)
+        h, c = eng.histograms()
+    check_hist(h, c, ho, co, kern, 'whole-sky sweep')
+    assert c.sum() > 200000
+
+
+@pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
 def test_adversarial_bin_edges_bit_exact(kern, var):
     """Pairs within a few ulps of an rt edge: the FP32 kernel must fall back to
     the FP64 formula and land where the oracle does."""
