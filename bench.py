@@ -11,11 +11,23 @@ search (work queue) + the per-slot histograms (W, DW, counts, RP, RT, Z) in
 one persistent launch.  Workload: the 150,000-forest synthetic catalogue
 (8,000 deg^2, 50x50 bins to 200 Mpc/h).  With N GPUs every rank bins its own
 catalogue of that size (different seed): weak scaling, no data-path
-collective.
+collective.  ``--split`` instead shares one catalogue among the N ranks as
+the drop-in drivers do: every rank holds the whole catalogue and neighbour
+queue, keeps the pairs of its LPT share of the owner pixels
+(``lya_select_slots``) and bins them (strong scaling, no data-path
+collective); its step is neighbour search + share selection + histograms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --profile-case corr|dist|adjoint [--config C] [--scale S]
 
-Prints one JSON line (rank 0).
+``--profile-case`` runs one pass of one hot kernel on a catalogue of the
+given configuration and scale (after one warm-up pass) and prints the
+library's statistics: the command line the ncu captures under ``profiles/``
+profile, on cases whose inputs exceed L2 while holding a few GB at most.
+
+Prints one JSON line (rank 0).  Its ``roofline`` is the pair kernel's FP32
+issue bound (the kernel is neither HBM- nor tensor-bound); the HBM figure and
+the shared-atomic term sit inside it as sub-objects.
 """
 import argparse
 import json
@@ -48,15 +60,24 @@ def parse():
     ap.add_argument('--config', type=int, default=1)
     ap.add_argument('--scale', type=float, default=1.0)
     ap.add_argument('--kernel', default='fp32', choices=list(KERNEL_CODES))
+    ap.add_argument('--split', action='store_true',
+                    help='share one catalogue among the ranks by owner pixel (strong scaling)')
     ap.add_argument('--e2e-steps', type=int, default=2)
     ap.add_argument('--cpu-seconds', type=float, default=15.0, help='target CPU-baseline sample duration')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-compare', action='store_true', help='skip the FP64 comparison sample')
+    ap.add_argument('--no-full-compare', action='store_true',
+                    help='skip the whole-catalogue FP64 runs of the comparison (about a minute)')
+    ap.add_argument('--no-ref-kernel', action='store_true',
+                    help="skip timing the reference's own CUDA kernel (oracle/_ref) on the comparison sample")
     ap.add_argument('--no-autotune', action='store_true', help='library default walk instead of the autotuned one')
     ap.add_argument('--dist-scale', type=float, default=0.03,
                     help='distortion sample: fraction of the 30,000-forest distortion catalogue (0 = skip)')
     ap.add_argument('--no-adjoint', action='store_true', help='skip the adjoint timing')
     ap.add_argument('--no-covariance', action='store_true', help='skip the covariance post-processing timing')
+    ap.add_argument('--profile-case', choices=['corr', 'dist', 'adjoint'], default=None,
+                    help='one pass of one hot kernel (after a warm-up pass), for profilers')
+    ap.add_argument('--variant', type=int, default=0, help='--profile-case corr: walk variant')
     return ap.parse_args()
 
 
@@ -195,6 +216,8 @@ def cpu_baseline(fs, angmax, seconds, seed=5):
 
 
 def build_catalog(config, scale, rank):
+    """The catalogue of ``rank``: its own seed (weak scaling), or rank 0's for
+    every rank when ``rank`` is 0 (the shared catalogue of ``--split``)."""
     from lya2pcf_b200 import synthetic
     seed = synthetic.SEEDS[config] + 1000 * rank
     fs = synthetic.make(config, scale=scale, seed=seed)
@@ -239,9 +262,17 @@ def run_b200(args, dist):
 
     dev = dist.local
     torch.cuda.set_device(dev)
-    fs, angmax = build_catalog(args.config, args.scale, dist.rank)
+    fs, angmax = build_catalog(args.config, args.scale, 0 if args.split else dist.rank)
     kern = KERNEL_CODES[args.kernel]
     eng = PairEngine(device=dev).upload(fs)
+    share = None
+    if args.split:
+        from lya2pcf_b200.sharding import shard_slots, slot_costs
+        eng.build_pairs(angmax)
+        f1, f2 = eng.get_pairs()
+        costs = slot_costs(fs.lengths, f1, f2, eng.slot_of_forest, len(eng.slot_pixels))
+        share = shard_slots(costs, dist.world)[dist.rank]
+        share_frac = float(costs[share].sum() / max(costs.sum(), 1.0))
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json')))
@@ -250,6 +281,8 @@ def run_b200(args, dist):
 
     def step():
         eng.build_pairs(angmax)
+        if share is not None:
+            eng.select_slots(share)
         return eng.run(kernel=kern, guard=GUARD)
 
     tune = None
@@ -304,10 +337,13 @@ def run_b200(args, dist):
                                      p(host['ra']), p(host['dec']), p(host['name']), p(host['slot']), nslot,
                                      p(host['omega']), p(host['odl2'])), eng.ctx)
         eng.build_pairs(angmax)
+        if share is not None:
+            eng.select_slots(share)
         eng.run(kernel=kern, guard=GUARD)
         N.check(L.lya_corr_get(eng.ctx, 0, nslot, p(hist_out), p(cnt_out)), eng.ctx)
 
     e2e_value = None
+    e2e_phases = None
     if args.e2e_steps > 0:
         e2e_step()
         dist.barrier()
@@ -318,6 +354,9 @@ def run_b200(args, dist):
         torch.cuda.synchronize()
         e2e_s = dist.max(time.perf_counter() - t)
         e2e_value = dist.sum(ref_pairs * args.e2e_steps) / e2e_s
+        e2e_phases = e2e_itemised(eng, e2e_step_parts(L, eng, fs, host, nslot, hist_out, cnt_out, angmax, kern,
+                                                      share))
+        e2e_phases['wall_ms_per_step'] = 1e3 * e2e_s / args.e2e_steps
 
     # ---- covariance of the per-owner-pixel correlations of the last run (post-processing, on the device)
     covariance = None
@@ -355,25 +394,30 @@ def run_b200(args, dist):
         # ---- FP32 vs FP64 on a sample of owner slots: bit-exact counts and pairs/s
         compare = None
         if not args.no_compare:
-            compare = fp64_comparison(eng, fs, kern)
-        # ---- roofline of the dominant kernel (the pair kernel)
+            compare = fp64_comparison(eng, fs, kern, full=not args.no_full_compare,
+                                      ref_kernel=not args.no_ref_kernel)
+        # ---- roofline of the dominant kernel (the pair kernel): FP32 issue bound
         kms = float(np.median(kernel_ms))
+        roof = alu_roofline(st, kms, clk)
         algo_bytes = st['ref_pixels'] * 24.0          # dc, w, dw (FP64) of both forests per forest pair
-        achieved = algo_bytes / (kms * 1e-3) / 1e9
+        achieved_gbs = algo_bytes / (kms * 1e-3) / 1e9
         hbm = peaks.get('hbm_gbs')
-        traffic = dram_traffic_per_launch(st['ref_pairs'])
-        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': hbm if hbm else 6650.0, 'unit': 'GB/s',
-                'frac': achieved / (hbm if hbm else 6650.0), 'traffic': traffic,
-                'peak_source': 'measured' if hbm else 'fallback',
-                'kernel': 'k_corr<FP32_GUARDED> (pair kernel)', 'kernel_ms': kms,
-                'algorithmic_bytes_per_launch': algo_bytes,
-                'note': 'not HBM-bound: the forests are re-read from L2; the bound is FP32 issue (see alu)',
-                'alu': alu_roofline(st, kms, clk)}
+        roof['traffic'] = dram_traffic_per_launch(st['ref_pairs'])
+        roof['kernel'] = 'k_corr<FP32_GUARDED> (pair kernel, lean walk)'
+        roof['kernel_ms'] = kms
+        roof['hbm'] = {'bound': 'hbm', 'achieved': achieved_gbs, 'peak': hbm if hbm else 6650.0, 'unit': 'GB/s',
+                       'frac': achieved_gbs / (hbm if hbm else 6650.0),
+                       'peak_source': 'measured (MEASURED_PEAKS.json)' if hbm else 'fallback',
+                       'algorithmic_bytes_per_launch': algo_bytes,
+                       'note': 'not the bound: per forest pair the kernel reads (len1+len2) x 24 B algorithmically, '
+                               're-read from L2'}
+        roof['smem_atomic'] = smem_atomic_term(st, kms)
         cpu = None if args.no_cpu_baseline else cpu_baseline(fs, angmax, args.cpu_seconds)
         distortion = None if args.dist_scale <= 0 else distortion_sample(args.dist_scale, dev)
         ms_step = t_max / args.steps
         out = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': dist.world, 'steps': args.steps,
-               'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+               'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True,
+               'scaling': 'strong' if args.split else 'weak',
                'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded catalogue, no public data set)',
                'config': {'workload': WORKLOAD, 'config': args.config, 'scale': args.scale, 'forests': fs.n,
                           'owner_pixels': nslot, 'forest_pairs': st['n_pairs'],
@@ -381,9 +425,12 @@ def run_b200(args, dist):
                           'guard_bound_mpc_h': st['guard_bound'], 'l2': 'inputs larger than L2 '
                           f'({fs.npix_total * 52 / 1e9:.1f} GB resident catalogue)',
                           'step': 'device neighbour search + histogram run',
-                          'parallelism': f'weak: {dist.world} rank(s), one catalogue each'},
+                          'parallelism': (f'split: {dist.world} rank(s) share one catalogue by owner pixel (LPT on '
+                                          f'the pair count; rank 0 holds {share_frac:.3f} of it)') if args.split
+                          else f'weak: {dist.world} rank(s), one catalogue each'},
                'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
-                       'path': 'lya_upload_forests + lya_build_pairs + lya_corr_run + lya_corr_get, pinned host'},
+                       'path': 'lya_upload_forests + lya_build_pairs + lya_corr_run + lya_corr_get, pinned host',
+                       'phases': e2e_phases},
                'tuned': tune, 'kernel_ms_steps': kernel_ms, 'run_ms_steps': run_ms, 'build_ms_steps': build_ms,
                'distortion': distortion, 'adjoint': adjoint, 'covariance': covariance,
                'gpu_launches': int(launches),
@@ -392,6 +439,40 @@ def run_b200(args, dist):
                'guard_fraction': st['guard_rechecks'] / max(st['evaluated_pairs'], 1.0),
                'roofline': roof, 'clocks': clk, 'cpu_baseline': cpu, 'fp64_comparison': compare}
     eng.close()
+    return out
+
+
+def e2e_step_parts(L, eng, fs, host, nslot, hist_out, cnt_out, angmax, kern, share=None):
+    """The four C-ABI calls of one end-to-end step, as separate callables."""
+    from lya2pcf_b200 import _native as N
+    p = N.ptr
+    return [
+        ('upload', lambda: N.check(L.lya_upload_forests(
+            eng.ctx, fs.n, p(host['start']), p(host['dc']), p(host['w']), p(host['dw']), p(host['z']), p(host['dl']),
+            p(host['ux']), p(host['uy']), p(host['uz']), p(host['ra']), p(host['dec']), p(host['name']),
+            p(host['slot']), nslot, p(host['omega']), p(host['odl2'])), eng.ctx)),
+        ('build_pairs', lambda: (eng.build_pairs(angmax), eng.select_slots(share) if share is not None else None)),
+        ('run', lambda: eng.run(kernel=kern, guard=GUARD)),
+        ('get', lambda: N.check(L.lya_corr_get(eng.ctx, 0, nslot, p(hist_out), p(cnt_out)), eng.ctx)),
+    ]
+
+
+def e2e_itemised(eng, parts):
+    """One more end-to-end step with each call bracketed by device events on
+    the library's stream (timer_start / timer_stop) and the host clock: where
+    an end-to-end step's time goes."""
+    out = {}
+    for name, fn in parts:
+        eng.sync()
+        t = time.perf_counter()
+        eng.timer_start()
+        fn()
+        dev_ms = eng.timer_stop()
+        out[name] = {'device_ms': dev_ms, 'wall_ms': 1e3 * (time.perf_counter() - t)}
+    out['sum_wall_ms'] = sum(v['wall_ms'] for v in out.values())
+    st = eng.stats()
+    out['run_kernel_ms'] = st['kernel_ms']
+    out['build_kernels_ms'] = st['build_ms']
     return out
 
 
@@ -417,8 +498,35 @@ def distortion_sample(scale, dev):
             'matrix': f'{D.shape[0]}x{D.shape[1]} float64, {int(np.count_nonzero(D))} nonzero'}
 
 
-def fp64_comparison(eng, fs, kern):
-    """FP32-guarded vs FP64 kernels on the same slots: counts must be equal."""
+XI_FLOOR_FRAC = 0.1   # per-bin xi errors are stated over bins with |xi| >= this fraction of the median |xi|
+
+
+def xi_errors(h32, h64):
+    """Error of xi = DW/W of the FP32-guarded histograms against the FP64
+    kernel's (which equals the oracle to 1e-12 in the tests), per owner pixel
+    and bin: normwise (max |dxi| / max |xi|) and per bin (|dxi| / |xi|) over the
+    bins whose |xi| is at least XI_FLOOR_FRAC of the median nonzero |xi|."""
+    W32, W64 = h32[:, 0], h64[:, 0]
+    xi32 = np.divide(h32[:, 1], W32, out=np.zeros_like(W32), where=W32 != 0)
+    xi64 = np.divide(h64[:, 1], W64, out=np.zeros_like(W64), where=W64 != 0)
+    d = np.abs(xi32 - xi64)
+    a = np.abs(xi64)
+    nz = a > 0
+    floor = XI_FLOOR_FRAC * float(np.median(a[nz])) if nz.any() else 0.0
+    sel = a >= floor if nz.any() else nz
+    rel = d[sel] / a[sel] if sel.any() else np.zeros(1)
+    return {'normwise_max_dxi_over_max_xi': float(d.max() / max(a.max(), 1e-300)),
+            'per_bin_floor_xi': floor, 'per_bin_floor_rule': f'|xi| >= {XI_FLOOR_FRAC} x median nonzero |xi|',
+            'per_bin_bins': int(sel.sum()), 'per_bin_max_rel_err': float(rel.max()),
+            'per_bin_median_rel_err': float(np.median(rel)),
+            'per_bin_fraction_within_1e-6': float(np.mean(rel <= 1e-6))}
+
+
+def fp64_comparison(eng, fs, kern, full=True, ref_kernel=True):
+    """FP32-guarded vs the FP64 kernels: a 40-owner-pixel sample (accuracy,
+    counts, pairs/s, and the reference's own CUDA kernel on the same pixels
+    when oracle/_ref was built), then the whole catalogue once per kernel
+    (counts equal in every bin of every pixel, and the speed-ups)."""
     from lya2pcf_b200.engine import owner_slots
     slot, pixels = owner_slots(fs.pix)
     nslot = len(pixels)
@@ -444,15 +552,64 @@ def fp64_comparison(eng, fs, kern):
     h32, h64 = hists['fp32_guarded'], hists['fp64_plain']
     W32, W64 = h32[:, 0], h64[:, 0]
     nz = W64 > 0
-    xi32 = np.divide(h32[:, 1], W32, out=np.zeros_like(W32), where=W32 != 0)
-    xi64 = np.divide(h64[:, 1], W64, out=np.zeros_like(W64), where=W64 != 0)
     res['max_rel_err_W'] = float(np.max(np.abs(W32 - W64)[nz] / W64[nz])) if nz.any() else 0.0
     res['max_rel_err_RP_RT_Z'] = [float(np.max(np.abs(h32[:, q] - h64[:, q])[nz] / np.abs(h64[:, q])[nz]))
                                   for q in (2, 3, 4)] if nz.any() else None
-    res['max_err_xi_over_max_xi'] = float(np.abs(xi32 - xi64).max() / max(np.abs(xi64).max(), 1e-300))
+    res['xi'] = xi_errors(h32, h64)
     res['speedup_fp32_vs_fp64plain'] = res['fp32_guarded']['pairs_per_s'] / res['fp64_plain']['pairs_per_s']
     res['speedup_fp32_vs_fp64diag'] = res['fp32_guarded']['pairs_per_s'] / res['fp64_diagonal']['pairs_per_s']
+    if ref_kernel:
+        res['reference_kernel'] = reference_kernel_sample(eng, fs, rngs, counts['fp64_plain'])
+        rk = res['reference_kernel']
+        if rk and rk.get('pairs_per_s'):
+            res['speedup_fp32_vs_reference_kernel'] = res['fp32_guarded']['pairs_per_s'] / rk['pairs_per_s']
+    if full:
+        res['whole_catalogue'] = whole_catalogue_comparison(eng)
     return res
+
+
+def whole_catalogue_comparison(eng):
+    """Every owner pixel of the catalogue with each kernel once: pixel pairs
+    per second from the kernel events, and pair counts of the FP64 kernels
+    equal to the FP32-guarded kernel's in every bin of every pixel."""
+    out = {}
+    c32 = None
+    for name, code in (('fp32_guarded', 0), ('fp64_diagonal', 1), ('fp64_plain', 2)):
+        st = eng.run(kernel=code, guard=GUARD)
+        _, c = eng.histograms()
+        out[name] = {'kernel_ms': st['kernel_ms'], 'pairs_per_s': st['run_ref_pairs'] / (st['kernel_ms'] * 1e-3),
+                     'evaluated_pairs': st['evaluated_pairs']}
+        if c32 is None:
+            c32 = c
+        else:
+            out[f'counts_equal_fp32_{name}'] = bool(np.array_equal(c32, c))
+    out['ref_pairs'] = st['run_ref_pairs']
+    out['speedup_fp32_vs_fp64plain'] = out['fp32_guarded']['pairs_per_s'] / out['fp64_plain']['pairs_per_s']
+    out['speedup_fp32_vs_fp64diag'] = out['fp32_guarded']['pairs_per_s'] / out['fp64_diagonal']['pairs_per_s']
+    return out
+
+
+def reference_kernel_sample(eng, fs, rngs, counts64):
+    """The reference's own pair_correlation (cuda_kernels.cpp:90-162, compiled
+    from the reference tree into oracle/_ref) on the same owner pixels, driven
+    per first forest as two_point_per_pixel does
+    (correlation_procedures_pycuda.py:141-166): a baseline, not the product.
+    Its W must have as many nonzero bins as the FP64 kernel's counts."""
+    from oracle import ref as R
+    if not R.available():
+        return {'unavailable': 'oracle/_ref/libref_kernels.so was not built (needs the reference tree at build time)'}
+    f1, f2 = eng.get_pairs()
+    sel = (eng.slot_of_forest[f1] >= rngs[0]) & (eng.slot_of_forest[f1] < rngs[1])
+    f1, f2 = f1[sel], f2[sel]
+    firsts, starts = np.unique(f1, return_index=True)
+    ends = np.append(starts[1:], len(f1))
+    lists = [f2[a:b] for a, b in zip(starts, ends)]
+    L = fs.lengths.astype(np.float64)
+    ref_pairs = float(np.sum(L[f1] * L[f2]))
+    ms, w_hist, _ = R.corr_timed(fs, firsts, lists)
+    return {'pairs_per_s': ref_pairs / (ms * 1e-3), 'loop_ms': ms, 'ref_pairs': ref_pairs, 'launches': len(firsts),
+            'nonzero_bins_match': bool(np.array_equal(w_hist.ravel() != 0, counts64.sum(0) != 0)),
+            'what': 'reference pair_correlation, one launch + synchronize per first forest, FP64 global atomics'}
 
 
 def dram_traffic_per_launch(ref_pairs):
@@ -466,22 +623,85 @@ def dram_traffic_per_launch(ref_pairs):
 
 
 def alu_roofline(st, kms, clk):
-    """Pair evaluations per second against the FP32 issue bound: the FP32
-    operations one pixel pair needs (10 in the reference kernel,
-    cuda_kernels.cpp:142-155: rp sub+mul, rt add+mul, two bin scalings, two
-    weight products, two accumulations; 7 more for the count-free new outputs:
-    three products and four accumulations) at the B200's FP32 rate."""
+    """The pair kernel against its FP32 issue bound: evaluated pixel pairs per
+    second against the B200's FP32 lane rate divided by the FP32 operations one
+    pixel pair needs (10 in the reference kernel, cuda_kernels.cpp:142-155: rp
+    sub+mul, rt add+mul, two bin scalings, two weight products, two
+    accumulations; 7 more for the new outputs: three products and four
+    accumulations).  The lane rate is 148 SMs x 128 FP32 lanes x the SM clock
+    sampled during the timed steps (computed, not measured)."""
     evals = st['evaluated_pairs'] / (kms * 1e-3)
     sm_mhz = (clk or {}).get('sm_mhz') or 1965.0
     fp32_lanes = 148 * 128 * sm_mhz * 1e6        # FP32 lane-instructions per second
     ops = 17.0
     bound = fp32_lanes / ops
-    return {'pair_evals_per_s': evals, 'fp32_ops_per_pair': ops, 'bound_pair_evals_per_s': bound,
-            'frac': evals / bound, 'sm_mhz_used': sm_mhz}
+    return {'bound': 'fp32_issue', 'achieved': evals, 'peak': bound, 'unit': 'pair-evaluations/s',
+            'frac': evals / bound, 'fp32_ops_per_pair': ops, 'sm_mhz_used': sm_mhz,
+            'peak_source': 'computed: 148 SMs x 128 FP32 lanes x sampled SM clock / 17 ops per pair (not measured)'}
+
+
+def smem_atomic_term(st, kms):
+    """The shared-memory atomic term of the bound: the reference algorithm does
+    6 shared atomics (5 FP64 sums and a count) per in-range pixel pair; the
+    kernel does 6 per run of pairs that share a bin.  Peak atomic rate from the
+    committed probe measurement (profiles/smem_atomic_rate.json)."""
+    try:
+        prof = json.load(open(os.path.join(ROOT, 'profiles', 'smem_atomic_rate.json')))
+        rate = float(prof['f64_add_random_bins_per_s'])
+    except Exception:
+        return None
+    evals = max(st['evaluated_pairs'], 1.0)
+    f_in = st['in_range_pairs'] / evals
+    per_pair_ref = 6.0 * f_in
+    per_pair_kernel = 6.0 * st['runs_flushed'] / evals
+    return {'peak_atomics_per_s': rate, 'source': 'measured probe, FP64 shared atomicAdd into random bins of a '
+                                                  '2500-bin histogram (profiles/smem_atomic_rate.md)',
+            'in_range_fraction': f_in,
+            'bound_pair_evals_per_s_reference_form': rate / per_pair_ref if per_pair_ref else None,
+            'atomics_per_evaluated_pair': per_pair_kernel,
+            'bound_pair_evals_per_s_this_kernel': rate / per_pair_kernel if per_pair_kernel else None,
+            'atomic_time_fraction': (st['runs_flushed'] * 6.0 / rate) / (kms * 1e-3)}
+
+
+def profile_case(args):
+    """One pass of the pair kernel, the distortion kernel or the adjoint on a
+    catalogue of configuration ``args.config`` at ``args.scale``, after one
+    warm-up pass; prints the library's statistics as one JSON line."""
+    from lya2pcf_b200 import synthetic
+    from lya2pcf_b200.engine import PairEngine
+    fs = synthetic.make(args.config, scale=args.scale)
+    kern = KERNEL_CODES[args.kernel]
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.build_pairs(synthetic.angmax_for(fs))
+        if args.profile_case == 'dist':
+            eng.distortion()
+            eng.distortion()
+            st = eng.stats()
+        elif args.profile_case == 'adjoint':
+            eng.run(kernel=kern, guard=GUARD)
+            g = np.random.default_rng(4).normal(size=eng.nb)
+            eng.adjoint(g)
+            t = time.perf_counter()
+            eng.adjoint(g)
+            st = eng.stats()
+            st['adjoint_wall_s'] = time.perf_counter() - t
+        else:
+            eng.run(kernel=kern, guard=GUARD, variant=args.variant)
+            st = eng.run(kernel=kern, guard=GUARD, variant=args.variant)
+        st['npix_total'] = fs.npix_total
+        st['case'] = {'kernel': args.profile_case, 'config': args.config, 'scale': args.scale, 'forests': fs.n}
+        print(json.dumps(st), flush=True)
 
 
 def main():
     args = parse()
+    if args.split:   # the extras below describe one catalogue on one GPU; a split run measures the step only
+        args.no_compare = args.no_adjoint = args.no_covariance = True
+        args.dist_scale = 0.0
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.impl == 'reference':
         # the reference path is CPU code: rank 0 alone runs it, other ranks exit
         if int(os.environ.get('RANK', '0')) != 0:

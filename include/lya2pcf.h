@@ -134,6 +134,14 @@ int lya_build_pairs(lya_ctx* ctx, double angmax, double mumin, int64_t* n_pairs_
  * pairs (f1[k], f2[k]) grouped by f1 (f1 non-decreasing). */
 int lya_set_pairs(lya_ctx* ctx, int64_t n_pairs, const int32_t* f1, const int32_t* f2);
 
+/* Keep only the work-queue pairs whose first forest's owner slot s has
+ * keep[s] != 0 (keep: host array of n_slots flags); the queue stays grouped
+ * by f1 and the reference pair counts of lya_stats follow.  Takes the place
+ * of the reference's scatter of healpix pixels over MPI ranks
+ * (2pla.py:87,102): a rank keeps the owner pixels assigned to it (any subset,
+ * e.g. a cost-balanced one) and its runs bin only those. */
+int lya_select_slots(lya_ctx* ctx, const uint8_t* keep);
+
 /* Copy the current work queue to the host (n_pairs entries each). */
 int lya_get_pairs(lya_ctx* ctx, int32_t* f1, int32_t* f2);
 
@@ -206,14 +214,32 @@ int lya_covariance_smooth(lya_ctx* ctx, const double* cov, double* cov_smooth, i
  * reference FP64 formula (the FP64 plain kernel).  The only scratch is a
  * file-scope device array of 4096 bins (320 KB per GPU that loads the
  * library, kept until exit): np*nt above 4096 is rejected with LYA_ERR_ARG.
- * The first call on a device resolves the array's device address and should
- * come before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race.  stream: a cudaStream_t, or NULL for the default
- * stream.  The call is asynchronous on that stream. */
+ * The call makes `device` current itself (cudaSetDevice on the library's own,
+ * statically linked, CUDA runtime).  The first call on a device does that
+ * device's set-up (the array's device address, the kernels' shared-memory
+ * limit, kernel loading, the SM count) and should come before any stream
+ * capture; later calls make no set-up calls.  All calls share the array:
+ * calls that overlap on the GPU race.  stream: a cudaStream_t, or NULL for the
+ * default stream.  The call is asynchronous on that stream.
+ * Preconditions the call does not check (it reads the caller's device memory
+ * as given): start has n_forests+1 non-decreasing entries with start[0] = 0
+ * and dc, w, dw, z hold start[n_forests] pixels; ux, uy, uz hold n_forests
+ * entries; 0 <= f1[k], f2[k] < n_forests for k < n_pairs. */
 int lya_corr_pixel_noalloc(int device, const double* dc, const double* w, const double* dw, const double* z,
                            const int64_t* start, const double* ux, const double* uy, const double* uz,
                            const int32_t* f1, const int32_t* f2, int64_t n_pairs, double rpmax, double rtmax,
                            int32_t np, int32_t nt, double* hist, uint64_t* counts, void* stream);
+
+/* Test hooks for the failure paths (no counterpart in the reference).
+ * lya_debug_fail_alloc: the device allocation made after `after` more
+ * allocations of the library fails once (LYA_ERR_ALLOC from the call that
+ * made it); -1 disarms.  LYA2PCF_FAIL_ALLOC=<after> in the environment arms it
+ * when the library loads.  lya_debug_inject(ctx, 1): the next lya_corr_run's
+ * pair kernel raises its device error flag, and the run returns
+ * LYA_ERR_DEVICE as it does when the kernel finds a run record outside the
+ * histogram.  Neither touches memory it should not: the context stays usable. */
+int lya_debug_fail_alloc(int64_t after);
+int lya_debug_inject(lya_ctx* ctx, int32_t what);
 
 /* Device timer on the context's stream: op 0 records the start event, op 1
  * records the stop event, waits for it and writes the elapsed milliseconds. */

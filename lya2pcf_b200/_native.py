@@ -36,6 +36,9 @@ SIGNATURES = {
     'lya_build_pairs': ([P, C.c_double, C.c_double, C.POINTER(C.c_int64)], C.c_int),
     'lya_set_pairs': ([P, C.c_int64, P, P], C.c_int),
     'lya_get_pairs': ([P, P, P], C.c_int),
+    'lya_select_slots': ([P, P], C.c_int),
+    'lya_debug_fail_alloc': ([C.c_int64], C.c_int),
+    'lya_debug_inject': ([P, C.c_int32], C.c_int),
     'lya_corr_run': ([P, P], C.c_int),
     'lya_corr_get': ([P, C.c_int32, C.c_int32, P, P], C.c_int),
     'lya_corr_adjoint': ([P, P, P, P, C.c_int32], C.c_int),

@@ -10,11 +10,42 @@
 //     FP32 kernel: dc = dc_hi + dc_lo to ~2^-48 relative, so FP32 differences
 //     of comoving distances stay accurate to ~1e-5 Mpc/h.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
 
 #include "lya_internal.cuh"
 
 static thread_local std::string g_thread_err;
+
+// ------------------------------------------------------------------ test hooks
+// Allocation-failure hook: the device allocation made after `g_fail_alloc_in`
+// more allocations fails once with cudaErrorMemoryAllocation (-1 = never).
+// LYA2PCF_FAIL_ALLOC=<n> in the environment arms it when the library loads.
+static std::atomic<long long> g_fail_alloc_in{[] {
+  const char* v = getenv("LYA2PCF_FAIL_ALLOC");
+  return v && *v ? atoll(v) : -1ll;
+}()};
+
+bool lya_alloc_fault() {
+  long long n = g_fail_alloc_in.load();
+  while (n >= 0) {
+    if (g_fail_alloc_in.compare_exchange_weak(n, n - 1)) return n == 0;
+  }
+  return false;
+}
+
+extern "C" int lya_debug_fail_alloc(int64_t after) {
+  g_fail_alloc_in.store(after < 0 ? -1 : (long long)after);
+  return LYA_OK;
+}
+
+extern "C" int lya_debug_inject(lya_ctx* ctx, int32_t what) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_debug_inject: ctx is NULL");
+  if (what != 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_debug_inject: unknown hook %d", what);
+  ctx->inject_device_error = true;
+  return LYA_OK;
+}
 
 int lya_fail(lya_ctx* ctx, int code, const char* fmt, ...) {
   char buf[1024];
@@ -39,6 +70,64 @@ void lya_free_catalog(DevCatalog& c) {
 void lya_free_queue(WorkQueue& q) {
   lya_free(q.f1); lya_free(q.f2);
   q = WorkQueue{};
+}
+
+static void free_staging(UploadStaging& t) {
+  lya_free(t.dc); lya_free(t.w); lya_free(t.dw); lya_free(t.z); lya_free(t.dl); lya_free(t.start);
+  lya_free(t.zero_w);
+  t = UploadStaging{};
+}
+
+void lya_free_nbr_scratch(NbrScratch& s) {
+  lya_free(s.band); lya_free(s.band2); lya_free(s.sidx); lya_free(s.sidx2); lya_free(s.sra); lya_free(s.sra2);
+  lya_free(s.bstart); lya_free(s.counts); lya_free(s.offsets); lya_free(s.flag); lya_free(s.tot);
+  if (s.tmp) cudaFree(s.tmp);
+  if (s.h_out) cudaFreeHost(s.h_out);
+  if (s.ev0) cudaEventDestroy(s.ev0);
+  if (s.ev1) cudaEventDestroy(s.ev1);
+  s = NbrScratch{};
+}
+
+// Device arrays of a catalogue of n forests and npad padded pixel slots.  The
+// arrays of the previous upload are kept when they are large enough, so that
+// uploading a catalogue of the same size again allocates and frees nothing
+// (and the buffers a captured run reads keep their addresses).
+static cudaError_t catalog_reserve(DevCatalog& c, int64_t n, int64_t npad) {
+  if (c.pstart && n <= c.cap_n && npad <= c.cap_npad) return cudaSuccess;
+  lya_free_catalog(c);
+  cudaError_t e = cudaSuccess;
+#define ALLOC(p, cnt) if (e == cudaSuccess) e = lya_alloc(&(p), (size_t)(cnt))
+  ALLOC(c.pstart, n); ALLOC(c.len, n); ALLOC(c.sorted, n); ALLOC(c.slot, n);
+  ALLOC(c.ux, n); ALLOC(c.uy, n); ALLOC(c.uz, n); ALLOC(c.ra, n); ALLOC(c.dec, n); ALLOC(c.name, n);
+  ALLOC(c.omega, n); ALLOC(c.odl2, n);
+  ALLOC(c.dc, npad); ALLOC(c.w, npad); ALLOC(c.dw, npad); ALLOC(c.z, npad); ALLOC(c.dl, npad);
+  ALLOC(c.pix4, npad); ALLOC(c.z32, npad); ALLOC(c.pix8, npad);
+#undef ALLOC
+  if (e != cudaSuccess) {
+    lya_free_catalog(c);
+    return e;
+  }
+  c.cap_n = n;
+  c.cap_npad = npad;
+  return cudaSuccess;
+}
+
+// Staging arrays for an upload of n forests and npix pixels (kept between uploads).
+static cudaError_t staging_reserve(UploadStaging& t, int64_t n, int64_t npix) {
+  if (t.start && n <= t.cap_n && npix <= t.cap_npix) return cudaSuccess;
+  free_staging(t);
+  cudaError_t e = cudaSuccess;
+#define ALLOC(p, cnt) if (e == cudaSuccess) e = lya_alloc(&(p), (size_t)(cnt))
+  ALLOC(t.dc, npix); ALLOC(t.w, npix); ALLOC(t.dw, npix); ALLOC(t.z, npix); ALLOC(t.dl, npix);
+  ALLOC(t.start, n + 1); ALLOC(t.zero_w, 1);
+#undef ALLOC
+  if (e != cudaSuccess) {
+    free_staging(t);
+    return e;
+  }
+  t.cap_n = n;
+  t.cap_npix = npix;
+  return cudaSuccess;
 }
 
 cudaError_t lya_queue_reserve(WorkQueue& q, int64_t n) {
@@ -102,7 +191,14 @@ extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   lya_free_catalog(ctx->cat);
+  free_staging(ctx->stg);
   lya_free_queue(ctx->wq);
+  lya_free_nbr_scratch(ctx->nbr);
+  lya_free(ctx->sel.keep); lya_free(ctx->sel.pos); lya_free(ctx->sel.o1); lya_free(ctx->sel.o2);
+  lya_free(ctx->sel.tot);
+  if (ctx->sel.tmp) cudaFree(ctx->sel.tmp);
+  if (ctx->sel.h_out) cudaFreeHost(ctx->sel.h_out);
+  lya_free(ctx->get_tmp);
   lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
   lya_free(ctx->cost);
   lya_free(ctx->cov);
@@ -261,8 +357,7 @@ static int upload_impl(lya_ctx* ctx, int64_t n, const int64_t* start, const doub
   if (npix > 0 && (!dc || !w || !dw || !z)) return lya_fail(ctx, LYA_ERR_ARG, "lya_upload_forests: pixel array NULL");
   LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
   LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  lya_free_catalog(ctx->cat);
-  lya_free_queue(ctx->wq);
+  ctx->wq.n_pairs = 0;   // the queue's buffers are kept for the next build
   ctx->have_result = false;
 
   ctx->h_start.assign(start, start + n + 1);
@@ -274,29 +369,21 @@ static int upload_impl(lya_ctx* ctx, int64_t n, const int64_t* start, const doub
     off += ((start[f + 1] - start[f]) + 3) & ~int64_t(3);
   }
   const int64_t npad = off + LYA_MARGIN;
+  cudaError_t e = catalog_reserve(ctx->cat, n, npad);
+  if (e == cudaSuccess) e = staging_reserve(ctx->stg, n, npix);
+  if (e != cudaSuccess) {
+    lya_free_catalog(ctx->cat);
+    free_staging(ctx->stg);
+    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_upload_forests: device allocation failed (%s)", cudaGetErrorString(e));
+  }
   DevCatalog& c = ctx->cat;
   c.n = n; c.npix = npix; c.npad = npad; c.n_slots = n_slots;
   c.has_dl = dl != nullptr;
   c.has_moments = (omega != nullptr && odl2 != nullptr) || ingest >= 0;
-
-  cudaError_t e = cudaSuccess;
-#define ALLOC(p, cnt) if (e == cudaSuccess) e = lya_alloc(&(p), (size_t)(cnt))
-  ALLOC(c.pstart, n); ALLOC(c.len, n); ALLOC(c.sorted, n); ALLOC(c.slot, n);
-  ALLOC(c.ux, n); ALLOC(c.uy, n); ALLOC(c.uz, n); ALLOC(c.ra, n); ALLOC(c.dec, n); ALLOC(c.name, n);
-  ALLOC(c.omega, n); ALLOC(c.odl2, n);
-  ALLOC(c.dc, npad); ALLOC(c.w, npad); ALLOC(c.dw, npad); ALLOC(c.z, npad); ALLOC(c.dl, npad);
-  ALLOC(c.pix4, npad); ALLOC(c.z32, npad); ALLOC(c.pix8, npad);
-  double *t_dc = nullptr, *t_w = nullptr, *t_dw = nullptr, *t_z = nullptr, *t_dl = nullptr;
-  int64_t* t_start = nullptr;
-  ALLOC(t_dc, npix); ALLOC(t_w, npix); ALLOC(t_dw, npix); ALLOC(t_z, npix); ALLOC(t_start, n + 1);
-  if (dl) ALLOC(t_dl, npix);
-#undef ALLOC
-  auto cleanup_tmp = [&]() { lya_free(t_dc); lya_free(t_w); lya_free(t_dw); lya_free(t_z); lya_free(t_dl); lya_free(t_start); };
-  if (e != cudaSuccess) {
-    cleanup_tmp();
-    lya_free_catalog(ctx->cat);
-    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_upload_forests: device allocation failed (%s)", cudaGetErrorString(e));
-  }
+  c.n_not_lean = 0;
+  double *t_dc = ctx->stg.dc, *t_w = ctx->stg.w, *t_dw = ctx->stg.dw, *t_z = ctx->stg.z;
+  double* t_dl = dl ? ctx->stg.dl : nullptr;
+  int64_t* t_start = ctx->stg.start;
   cudaStream_t s = ctx->stream;
   auto H2D = [&](void* d, const void* h, size_t bytes) {
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
@@ -324,8 +411,8 @@ static int upload_impl(lya_ctx* ctx, int64_t n, const int64_t* start, const doub
   if (e == cudaSuccess && !odl2) e = cudaMemsetAsync(c.odl2, 0, sizeof(double) * n, s);
   unsigned long long* zero_w = nullptr;
   if (e == cudaSuccess && ingest >= 0 && n > 0) {
-    e = lya_alloc(&zero_w, 1);
-    if (e == cudaSuccess) e = cudaMemsetAsync(zero_w, 0, sizeof(unsigned long long), s);
+    zero_w = ctx->stg.zero_w;
+    e = cudaMemsetAsync(zero_w, 0, sizeof(unsigned long long), s);
     if (e == cudaSuccess) {
       const int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
       k_project<<<blocks, 128, 0, s>>>(n, t_start, t_w, t_dw, t_dl, c.omega, c.odl2, ingest, zero_w);
@@ -346,8 +433,6 @@ static int upload_impl(lya_ctx* ctx, int64_t n, const int64_t* start, const doub
   if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(flags.data(), c.sorted, (size_t)n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && zero_w) e = cudaMemcpyAsync(&nzero, zero_w, sizeof(nzero), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  lya_free(zero_w);
-  cleanup_tmp();
   if (e == cudaSuccess && nzero) {
     lya_free_catalog(ctx->cat);
     return lya_fail(ctx, LYA_ERR_DATA, "lya_upload_deltas: %llu forests have weights summing to 0", nzero);
@@ -534,9 +619,16 @@ extern "C" int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double*
   LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
   const int nb = ctx->hist_nb;
   if (hist) {
-    double* tmp = nullptr;
-    cudaError_t e = lya_alloc(&tmp, (size_t)n * LYA_NQ * nb);
-    if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_get: device allocation failed");
+    const int64_t need = (int64_t)n * LYA_NQ * nb;
+    if (ctx->get_tmp_cap < need) {   // kept for later calls
+      lya_free(ctx->get_tmp);
+      ctx->get_tmp_cap = 0;
+      if (lya_alloc(&ctx->get_tmp, (size_t)need) != cudaSuccess)
+        return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_get: device allocation failed");
+      ctx->get_tmp_cap = need;
+    }
+    double* tmp = ctx->get_tmp;
+    cudaError_t e = cudaSuccess;
     const double* src = ctx->hist + (size_t)slot_first * LYA_NQ * 2 * nb;
     int blocks = (int)std::min<int64_t>(((int64_t)n * LYA_NQ * nb + 255) / 256, (int64_t)ctx->num_sms * 8);
     k_combine<<<blocks, 256, 0, ctx->stream>>>(n, nb, src, tmp);
@@ -545,7 +637,6 @@ extern "C" int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double*
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(hist, tmp, sizeof(double) * (size_t)n * LYA_NQ * nb, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    lya_free(tmp);
     if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_get: %s", cudaGetErrorString(e));
   }
   if (counts) {
@@ -582,6 +673,7 @@ extern "C" int lya_sync(lya_ctx* ctx) {
 
 extern "C" int lya_stats(lya_ctx* ctx, lya_stats_t* out) {
   if (!ctx || !out) return lya_fail(ctx, LYA_ERR_ARG, "lya_stats: NULL argument");
+  lya_resolve_build_timing(ctx);
   *out = ctx->last;
   out->launches = ctx->launches;
   out->n_pairs = ctx->wq.n_pairs;

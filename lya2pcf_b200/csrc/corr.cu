@@ -70,6 +70,7 @@ struct CorrParams {
   int cos_variant;
   int run_cap;
   int variant;          // walk: 0 default, 1 one diagonal per lane, 2 two diagonals per lane
+  int inject_error;     // test hook: block 0 raises the device error flag (lya_debug_inject)
   double* hist;                 // [slot][LYA_NQ][2][nb]
   unsigned long long* counts;   // [slot][nb]
   unsigned long long* stats;    // [ST_N]
@@ -84,6 +85,7 @@ struct SmemHist {
   double* q;                  // [LYA_NQ][nb]
   unsigned int* n;            // [nb] pair counts (native 32-bit shared atomics)
   unsigned long long* gc;     // [nb] global counts of the slot being accumulated
+  unsigned long long* err;    // device error flags (stats[ST_ERROR]): bit 0 = a record outside the histogram
 };
 
 // Count n more pairs in bin b: a 32-bit shared counter whose wrap-around is
@@ -169,6 +171,10 @@ __device__ __forceinline__ void drain(Rec* buf, int cnt, const SmemHist& h, int 
   __syncwarp();
   for (int k = lane; k < cnt; k += 32) {
     const Rec r = buf[k];
+    if ((unsigned)r.bin >= (unsigned)nb || r.n <= 0) {   // never written by a correct walk: report, skip
+      atomicOr(h.err, 1ull);
+      continue;
+    }
     st.runs++;
     st.inrange += (unsigned long long)r.n;
     atomicAdd(&h.q[0 * nb + r.bin], (double)r.aw);
@@ -1058,6 +1064,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_corr(const CorrParams p) {
   h.q = reinterpret_cast<double*>(smem);
   h.n = reinterpret_cast<unsigned int*>(h.q + LYA_NQ * nb);
   h.gc = nullptr;
+  h.err = p.stats + ST_ERROR;
+  if (p.inject_error && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(h.err, 2ull);
   // the count array keeps 8 bytes per bin so the record buffers stay 16-byte aligned
   unsigned char* bufs = reinterpret_cast<unsigned char*>(h.q + LYA_NQ * nb) + (size_t)nb * sizeof(unsigned long long);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1370,6 +1378,8 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
   p.cos_variant = ctx->cos_variant;
   p.run_cap = o->run_cap > 0 ? o->run_cap : 128;
   p.variant = o->variant;
+  p.inject_error = ctx->inject_device_error ? 1 : 0;
+  ctx->inject_device_error = false;   // one run
   p.hist = ctx->hist; p.counts = ctx->counts; p.stats = ctx->stats;
   key.kind = kind; key.nctas = nctas; key.nslots = nslots; key.nb = nb; key.n_items = n;
   key.slot_begin = o->slot_begin; key.slot_end = o->slot_end;
@@ -1428,6 +1438,12 @@ int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o) {
   ctx->last.guard_rechecks = (double)hst[ST_RECHECK];
   ctx->last.runs_flushed = (double)hst[ST_RUNS];
   ctx->last.in_range_pairs = (double)hst[ST_INRANGE];
+  if (hst[ST_ERROR]) {
+    ctx->have_result = false;
+    return lya_fail(ctx, LYA_ERR_DEVICE, "lya_corr_run: the pair kernel raised its error flag 0x%llx (%s)",
+                    (unsigned long long)hst[ST_ERROR],
+                    (hst[ST_ERROR] & 1) ? "a run record outside the histogram was dropped" : "injected by lya_debug_inject");
+  }
   ctx->have_result = true;
   return LYA_OK;
 }

@@ -63,6 +63,43 @@ struct DevCatalog {
   bool has_dl = false;
   bool has_moments = false;
   int64_t n_not_lean = 0;      // forests without the LYA_LEAN flag
+  int64_t cap_n = 0;           // allocated forests of the per-forest arrays
+  int64_t cap_npad = 0;        // allocated padded pixel slots of the per-pixel arrays
+};
+
+// Staging of an upload: the caller's unpadded CSR arrays on the device, packed
+// into the DevCatalog by k_pack.  Kept between uploads (grown, never shrunk).
+struct UploadStaging {
+  double* dc = nullptr;
+  double* w = nullptr;
+  double* dw = nullptr;
+  double* z = nullptr;
+  double* dl = nullptr;
+  int64_t* start = nullptr;
+  unsigned long long* zero_w = nullptr;   // [1] forests whose weights sum to 0
+  int64_t cap_npix = 0, cap_n = 0;
+};
+
+// Scratch of the device neighbour search, kept between builds (grown, never
+// shrunk), so a build allocates nothing once sized.
+struct NbrScratch {
+  int32_t* band = nullptr;      // [cap_n] band of each forest, then the sorted bands
+  int32_t* band2 = nullptr;     // [cap_n]
+  int32_t* sidx = nullptr;      // [cap_n] forests in (band, ra) order
+  int32_t* sidx2 = nullptr;     // [cap_n]
+  double* sra = nullptr;        // [cap_n] their ra
+  double* sra2 = nullptr;       // [cap_n]
+  int64_t* bstart = nullptr;    // [cap_band + 1]
+  long long* counts = nullptr;  // [cap_n + 1]
+  long long* offsets = nullptr; // [cap_n + 1]
+  int* flag = nullptr;          // [1] some ra outside [0, 2 pi)
+  double* tot = nullptr;        // [2] sum len1*len2, sum len1+len2
+  void* tmp = nullptr;          // cub sort / scan scratch
+  size_t tmp_bytes = 0;
+  int64_t cap_n = 0, cap_band = 0;
+  long long* h_out = nullptr;   // pinned [4]: pair count, then tot as double bits
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // build timing, read lazily by lya_stats
+  bool timing_pending = false;
 };
 
 struct WorkQueue {
@@ -86,6 +123,20 @@ struct DistScratch {
   alignas(16) unsigned char key[512] = {};   // the kernel parameters it was captured with
 };
 
+// Scratch of lya_select_slots (kept between calls, grown, never shrunk).
+struct SelectScratch {
+  uint8_t* keep = nullptr;      // [keep_cap] slot keep flags
+  long long* pos = nullptr;     // [cap + 1] item flags, then their exclusive scan
+  int32_t* o1 = nullptr;        // [cap] compacted queue
+  int32_t* o2 = nullptr;
+  double* tot = nullptr;        // [2] reference pixel pairs and pixels of the kept items
+  void* tmp = nullptr;          // cub scan scratch
+  size_t tmp_bytes = 0;
+  int64_t cap = 0;
+  int32_t keep_cap = 0;
+  double* h_out = nullptr;      // pinned [3]: kept count (as long long bits), tot
+};
+
 struct lya_ctx {
   int device = 0;
   int num_sms = 148;
@@ -105,7 +156,11 @@ struct lya_ctx {
   std::vector<int64_t> h_pstart;
   std::vector<int32_t> h_slot;
 
+  UploadStaging stg;
+
   WorkQueue wq;
+  NbrScratch nbr;
+  SelectScratch sel;
   int cos_variant = 0;
 
   // correlation outputs: per slot, LYA_NQ quantities as (hi, lo) FP64 pairs,
@@ -114,6 +169,8 @@ struct lya_ctx {
   unsigned long long* counts = nullptr;  // [n_slots][nb]
   int32_t hist_slots = 0, hist_nb = 0;
   bool have_result = false;
+  double* get_tmp = nullptr;             // lya_corr_get's combined (hi + lo) sums, kept between calls
+  int64_t get_tmp_cap = 0;
 
   unsigned long long* stats = nullptr;   // [ST_N]
   int64_t* cta_begin = nullptr;          // [max ctas + 1]
@@ -131,6 +188,7 @@ struct lya_ctx {
   int64_t graph_launches = 0;            // runs replayed from the captured graph
 
   lya_stats_t last{};
+  bool inject_device_error = false;      // test hook: the next run's pair kernel raises its error flag
 
   DistScratch dist;
 
@@ -150,10 +208,15 @@ int lya_fail(lya_ctx* ctx, int code, const char* fmt, ...);
                                            cudaGetErrorString(e_));                         \
   } while (0)
 
+// Allocation-failure hook (lya_debug_fail_alloc, or LYA2PCF_FAIL_ALLOC in the
+// environment): true when this device allocation is the one to fail.
+bool lya_alloc_fault();
+
 template <typename T>
 inline cudaError_t lya_alloc(T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
+  if (lya_alloc_fault()) return cudaErrorMemoryAllocation;
   return cudaMalloc((void**)p, count * sizeof(T));
 }
 
@@ -165,6 +228,9 @@ inline void lya_free(T*& p) {
 
 void lya_free_catalog(DevCatalog& c);
 void lya_free_queue(WorkQueue& q);
+void lya_free_nbr_scratch(NbrScratch& s);
+// build_ms of the last neighbour build, once its stop event has completed
+void lya_resolve_build_timing(lya_ctx* ctx);
 // Room for n pairs in q (f1, f2), keeping the buffers when they are large
 // enough; n_pairs is left to the caller.
 cudaError_t lya_queue_reserve(WorkQueue& q, int64_t n);

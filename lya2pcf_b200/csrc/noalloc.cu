@@ -13,9 +13,13 @@
 // __device__ array, so it calls no cudaMalloc, cudaFree or allocating library
 // routine.  Consequences of the shared array:
 //   * every GPU that loads the library holds the 320 KB until the process exits;
-//   * the first call on a device looks the array's device address up
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture;
+//   * the first call on a device does that device's set-up with the device
+//     current: it looks the array's device address up (cudaGetSymbolAddress),
+//     raises the kernel's dynamic shared-memory limit to what 4096 bins need,
+//     loads both kernels and reads the SM count; later calls make none of
+//     these driver calls.  Make that first call before any stream capture;
+//   * the call selects the device itself (cudaSetDevice on the library's own,
+//     statically linked, CUDA runtime);
 //   * every call clears the part of the array it uses, but all calls share it:
 //     calls that overlap on the GPU (different streams or threads without
 //     ordering) race on it and give wrong sums.
@@ -115,8 +119,34 @@ __global__ void k_noalloc_combine(int nb, const double* __restrict__ acc, double
   }
 }
 
+// Per-device state of the set-up done by the first call on each device.
+struct DeviceSetup {
+  double* acc;   // device address of g_noalloc_acc on that device
+  int sms;       // multiprocessor count
+};
 std::mutex g_setup_mu;
-double* g_acc_addr[64] = {nullptr};
+DeviceSetup g_setup[64] = {};
+bool g_ready[64] = {};
+
+// Set-up of `device` (which is current): cudaGetSymbolAddress of the scratch,
+// the shared-memory limit for the largest binning, a first touch of both
+// kernels (so that no later call loads a kernel, even one that launches only
+// the combine step), and the SM count.
+cudaError_t setup_device(int device, DeviceSetup* out) {
+  DeviceSetup d = {nullptr, 148};
+  cudaError_t e = cudaGetSymbolAddress((void**)&d.acc, g_noalloc_acc);
+  if (e != cudaSuccess) return e;
+  const size_t smem_max = (size_t)LYA_NOALLOC_MAX_BINS * (LYA_NQ * sizeof(double) + sizeof(unsigned long long));
+  e = cudaFuncSetAttribute(k_corr_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa;
+  e = cudaFuncGetAttributes(&fa, k_noalloc_combine);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  *out = d;
+  return cudaSuccess;
+}
 
 }  // namespace
 
@@ -136,21 +166,21 @@ extern "C" int lya_corr_pixel_noalloc(int device, const double* dc, const double
   if (device < 0 || device >= 64) return lya_fail(nullptr, LYA_ERR_ARG, "lya_corr_pixel_noalloc: bad device");
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return lya_fail(nullptr, LYA_ERR_CUDA, "lya_corr_pixel_noalloc: %s", cudaGetErrorString(e));
-  double* acc = nullptr;
+  DeviceSetup dev;
   {
     // set-up once per device, with that device current: the device address of
-    // the scratch array (its host-side name is only a stand-in)
+    // the scratch array (its host-side name is only a stand-in) and the rest
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_acc_addr[device]) {
-      e = cudaGetSymbolAddress((void**)&g_acc_addr[device], g_noalloc_acc);
-      if (e != cudaSuccess) {
-        g_acc_addr[device] = nullptr;
-        return lya_fail(nullptr, LYA_ERR_CUDA, "lya_corr_pixel_noalloc: cudaGetSymbolAddress: %s",
+    if (!g_ready[device]) {
+      e = setup_device(device, &g_setup[device]);
+      if (e != cudaSuccess)
+        return lya_fail(nullptr, LYA_ERR_CUDA, "lya_corr_pixel_noalloc: set-up of device %d: %s", device,
                         cudaGetErrorString(e));
-      }
+      g_ready[device] = true;
     }
-    acc = g_acc_addr[device];
+    dev = g_setup[device];
   }
+  double* acc = dev.acc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nb = np * nt;
   e = cudaMemsetAsync(acc, 0, sizeof(double) * LYA_NQ * 2 * (size_t)nb, s);
@@ -161,15 +191,10 @@ extern "C" int lya_corr_pixel_noalloc(int device, const double* dc, const double
     p.n_pairs = n_pairs; p.binner_rp = (double)np / rpmax; p.binner_rt = (double)nt / rtmax;
     p.np = np; p.nt = nt; p.nb = nb; p.acc = acc; p.counts = reinterpret_cast<unsigned long long*>(counts);
     const size_t smem = (size_t)nb * (LYA_NQ * sizeof(double) + sizeof(unsigned long long));
-    e = cudaFuncSetAttribute(k_corr_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) {
-      int sms = 148;
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-      const int64_t want = (n_pairs + 7) / 8;
-      const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, sms));
-      k_corr_noalloc<<<blocks, 256, smem, s>>>(p);
-      e = cudaGetLastError();
-    }
+    const int64_t want = (n_pairs + 7) / 8;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, dev.sms));
+    k_corr_noalloc<<<blocks, 256, smem, s>>>(p);
+    e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     k_noalloc_combine<<<(LYA_NQ * nb + 255) / 256, 256, 0, s>>>(nb, acc, hist);

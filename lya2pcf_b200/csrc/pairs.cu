@@ -12,17 +12,16 @@
 // reference's exact membership test (FP64, Python's operation order, no FMA).
 // The pre-filter is a superset of the disc, so the neighbour set equals the
 // reference's; pairs are written grouped by f1 in forest order.
-#include <thrust/binary_search.h>
-#include <thrust/execution_policy.h>
-#include <thrust/iterator/counting_iterator.h>
-#include <thrust/iterator/zip_iterator.h>
-#include <thrust/scan.h>
-#include <thrust/sequence.h>
-#include <thrust/sort.h>
-#include <thrust/tuple.h>
+//
+// The build allocates nothing once its scratch is sized (the sorts and the scan
+// are cub calls on scratch kept in the context) and synchronises once, to size
+// the queue from the count pass.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "lya_internal.cuh"
 
@@ -30,16 +29,44 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-__global__ void k_bands(int64_t n, const double* __restrict__ ra, const double* __restrict__ dec, double band_h,
-                        int64_t nband, int32_t* __restrict__ band, double* __restrict__ ra_key,
+__device__ __forceinline__ int32_t band_of(double dec, double band_h, int64_t nband) {
+  int64_t b = (int64_t)floor((dec + M_PI_2) / band_h);
+  b = b < 0 ? 0 : (b >= nband ? nband - 1 : b);
+  return (int32_t)b;
+}
+
+__global__ void k_bands(int64_t n, const double* __restrict__ ra, double* __restrict__ ra_key,
                         int32_t* __restrict__ idx, int* __restrict__ ra_out_of_range) {
   for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < n; f += (int64_t)gridDim.x * blockDim.x) {
-    int64_t b = (int64_t)floor((dec[f] + M_PI_2) / band_h);
-    b = b < 0 ? 0 : (b >= nband ? nband - 1 : b);
-    band[f] = (int32_t)b;
     ra_key[f] = ra[f];
     idx[f] = (int32_t)f;
     if (!(ra[f] >= 0.0 && ra[f] < 2.0 * M_PI)) atomicExch(ra_out_of_range, 1);
+  }
+}
+
+// band of every forest, in the ra order of the first sort
+__global__ void k_band_keys(int64_t n, const int32_t* __restrict__ idx, const double* __restrict__ dec,
+                            double band_h, int64_t nband, int32_t* __restrict__ band) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    band[q] = band_of(dec[idx[q]], band_h, nband);
+}
+
+// ra in (band, ra) order
+__global__ void k_gather_ra(int64_t n, const int32_t* __restrict__ idx, const double* __restrict__ ra,
+                            double* __restrict__ sra) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    sra[q] = ra[idx[q]];
+}
+
+// bstart[b] = first position of band >= b in the sorted band array, b = 0..nband
+__global__ void k_band_starts(int64_t n, const int32_t* __restrict__ band, int64_t nband, int64_t* __restrict__ bstart) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b <= nband; b += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (band[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    bstart[b] = lo;
   }
 }
 
@@ -73,6 +100,8 @@ struct NbrParams {
   int64_t nband;
   double band_h, angmax, mumin;
   const int* ra_out_of_range;
+  const int32_t* len;         // forest lengths (count pass: reference pixel pairs)
+  double* tot;                // count pass: [0] += sum len1*len2, [1] += sum len1+len2
   long long* counts;          // count pass output
   const long long* offsets;   // fill pass input (exclusive scan of counts)
   int32_t* of1;
@@ -90,8 +119,7 @@ __global__ void k_neighbours(const NbrParams p) {
     const double ra1 = p.ra[f1], dec1 = p.dec[f1];
     const double x1 = p.ux[f1], y1 = p.uy[f1], z1 = p.uz[f1];
     const long long nm1 = p.name[f1];
-    int64_t b1 = (int64_t)floor((dec1 + M_PI_2) / p.band_h);
-    b1 = b1 < 0 ? 0 : (b1 >= p.nband ? p.nband - 1 : b1);
+    const int64_t b1 = band_of(dec1, p.band_h, p.nband);
     // right-ascension half-width of the disc: sin(dra/2) <= sin(angmax/2)/cos(|dec|+angmax)
     const double dlim = fabs(dec1) + p.angmax * (1.0 + 1e-6) + 1e-9;
     bool full = !all_in;
@@ -107,6 +135,8 @@ __global__ void k_neighbours(const NbrParams p) {
       }
     }
     long long cnt = 0;
+    double cost = 0.0, pix = 0.0;   // count pass: this lane's accepted pairs
+    const double l1 = FILL ? 0.0 : (double)p.len[f1];
     const long long base = FILL ? p.offsets[f1] : 0;
     for (int64_t b = b1 - 1; b <= b1 + 1; ++b) {
       if (b < 0 || b >= p.nband) continue;
@@ -138,6 +168,11 @@ __global__ void k_neighbours(const NbrParams p) {
             acc = mu > p.mumin && nm1 != p.name[f2] && ra1 < p.ra[f2];
           }
           const unsigned bal = __ballot_sync(FULL, acc);
+          if (!FILL && acc) {
+            const double l2 = (double)p.len[f2];
+            cost += l1 * l2;
+            pix += l1 + l2;
+          }
           if (FILL && acc) {
             const long long pos = base + cnt + __popc(bal & ((1u << lane) - 1u));
             p.of1[pos] = (int32_t)f1;
@@ -147,119 +182,199 @@ __global__ void k_neighbours(const NbrParams p) {
         }
       }
     }
-    if (!FILL && lane == 0) p.counts[f1] = cnt;
+    if (!FILL) {
+      // integer-valued sums below 2^53: exact in any order
+      for (int o = 16; o > 0; o >>= 1) {
+        cost += __shfl_xor_sync(FULL, cost, o);
+        pix += __shfl_xor_sync(FULL, pix, o);
+      }
+      if (lane == 0) {
+        p.counts[f1] = cnt;
+        if (cost != 0.0) atomicAdd(p.tot, cost);
+        if (pix != 0.0) atomicAdd(p.tot + 1, pix);
+      }
+    }
   }
 }
 
-// out[0] += sum len1*len2 (reference pixel pairs), out[1] += sum len1+len2
-__global__ void k_pair_cost(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ f2,
-                            const int32_t* __restrict__ len, double* __restrict__ out) {
-  double acc = 0.0, pix = 0.0;
+// keep flag of every work item: its first forest's owner slot is kept
+__global__ void k_keep_flags(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ slot,
+                             const uint8_t* __restrict__ keep, long long* __restrict__ flag) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    flag[k] = keep[slot[f1[k]]] ? 1 : 0;
+}
+
+// scatter the kept items to their compacted positions (pos = exclusive scan of
+// the flags, in the same buffer) and sum their reference pixel pairs
+__global__ void k_keep_scatter(int64_t n, const int32_t* __restrict__ f1, const int32_t* __restrict__ f2,
+                               const uint8_t* __restrict__ keep, const int32_t* __restrict__ slot,
+                               const long long* __restrict__ pos, const int32_t* __restrict__ len,
+                               int32_t* __restrict__ o1, int32_t* __restrict__ o2, double* __restrict__ tot) {
+  double cost = 0.0, pix = 0.0;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-    const double l1 = (double)len[f1[k]], l2 = (double)len[f2[k]];
-    acc += l1 * l2;
-    pix += l1 + l2;
+    const int32_t a = f1[k];
+    if (keep[slot[a]]) {
+      const int32_t b = f2[k];
+      o1[pos[k]] = a;
+      o2[pos[k]] = b;
+      const double l1 = (double)len[a], l2 = (double)len[b];
+      cost += l1 * l2;
+      pix += l1 + l2;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
-    acc += __shfl_xor_sync(FULL, acc, o);
+    cost += __shfl_xor_sync(FULL, cost, o);
     pix += __shfl_xor_sync(FULL, pix, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(out, acc);
-    atomicAdd(out + 1, pix);
+    if (cost != 0.0) atomicAdd(tot, cost);
+    if (pix != 0.0) atomicAdd(tot + 1, pix);
   }
 }
 
 }  // namespace
 
+// Scratch for a build over n forests and nband declination bands, kept
+// between builds when large enough.
+static cudaError_t nbr_reserve(lya_ctx* ctx, int64_t n, int64_t nband) {
+  NbrScratch& S = ctx->nbr;
+  cudaError_t e = cudaSuccess;
+  if (!S.h_out) {
+    e = cudaMallocHost((void**)&S.h_out, sizeof(long long) * 4);
+    if (e == cudaSuccess) e = cudaEventCreate(&S.ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&S.ev1);
+    if (e == cudaSuccess) e = lya_alloc(&S.flag, 1);
+    if (e == cudaSuccess) e = lya_alloc(&S.tot, 2);
+    if (e != cudaSuccess) return e;
+  }
+  if (S.band && n <= S.cap_n && nband <= S.cap_band) return cudaSuccess;
+  lya_free(S.band); lya_free(S.band2); lya_free(S.sidx); lya_free(S.sidx2); lya_free(S.sra); lya_free(S.sra2);
+  lya_free(S.bstart); lya_free(S.counts); lya_free(S.offsets);
+  if (S.tmp) cudaFree(S.tmp);
+  S.tmp = nullptr;
+  S.tmp_bytes = 0;
+  S.cap_n = 0;
+  S.cap_band = 0;
+  e = lya_alloc(&S.band, n);
+  if (e == cudaSuccess) e = lya_alloc(&S.band2, n);
+  if (e == cudaSuccess) e = lya_alloc(&S.sidx, n);
+  if (e == cudaSuccess) e = lya_alloc(&S.sidx2, n);
+  if (e == cudaSuccess) e = lya_alloc(&S.sra, n);
+  if (e == cudaSuccess) e = lya_alloc(&S.sra2, n);
+  if (e == cudaSuccess) e = lya_alloc(&S.bstart, nband + 1);
+  if (e == cudaSuccess) e = lya_alloc(&S.counts, n + 1);
+  if (e == cudaSuccess) e = lya_alloc(&S.offsets, n + 1);
+  // cub scratch: the larger of the two sorts and the scan
+  size_t b1 = 0, b2 = 0, b3 = 0;
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairs(nullptr, b1, S.sra2, S.sra, S.sidx2, S.sidx, (int)n, 0, 64, ctx->stream);
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairs(nullptr, b2, S.band2, S.band, S.sidx2, S.sidx, (int)n, 0, 32, ctx->stream);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, b3, S.counts, S.offsets, (int)(n + 1), ctx->stream);
+  const size_t bytes = std::max(b1, std::max(b2, b3));
+  if (e == cudaSuccess) e = cudaMalloc(&S.tmp, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) return e;
+  S.tmp_bytes = std::max<size_t>(bytes, 16);
+  S.cap_n = n;
+  S.cap_band = nband;
+  return cudaSuccess;
+}
+
+void lya_resolve_build_timing(lya_ctx* ctx) {
+  NbrScratch& S = ctx->nbr;
+  if (!S.timing_pending) return;
+  float ms = 0.f;
+  if (cudaEventSynchronize(S.ev1) == cudaSuccess && cudaEventElapsedTime(&ms, S.ev0, S.ev1) == cudaSuccess)
+    ctx->last.build_ms = ms;
+  S.timing_pending = false;
+}
+
 int lya_build_queue(lya_ctx* ctx, double angmax, double mumin) {
   const int64_t n = ctx->cat.n;
   cudaStream_t s = ctx->stream;
-  auto pol = thrust::cuda::par.on(s);
   const double h = angmax * (1.0 + 1e-6) + 1e-9;
   const int64_t nband = (int64_t)std::ceil(M_PI / h) + 2;
-
-  int32_t *band = nullptr, *sidx = nullptr;
-  double *sra = nullptr, *tot = nullptr;
-  int64_t* bstart = nullptr;
-  long long *counts = nullptr, *offsets = nullptr;
-  int* flag = nullptr;
-  cudaError_t e = lya_alloc(&band, n);
-  if (e == cudaSuccess) e = lya_alloc(&sidx, n);
-  if (e == cudaSuccess) e = lya_alloc(&sra, n);
-  if (e == cudaSuccess) e = lya_alloc(&bstart, nband + 1);
-  if (e == cudaSuccess) e = lya_alloc(&counts, n + 1);
-  if (e == cudaSuccess) e = lya_alloc(&offsets, n + 1);
-  if (e == cudaSuccess) e = lya_alloc(&flag, 1);
-  if (e == cudaSuccess) e = lya_alloc(&tot, 2);
-  auto cleanup = [&]() {
-    lya_free(band); lya_free(sidx); lya_free(sra); lya_free(bstart); lya_free(counts); lya_free(offsets);
-    lya_free(flag); lya_free(tot);
-  };
+  if (n >= (int64_t)INT32_MAX - 1) return lya_fail(ctx, LYA_ERR_ARG, "lya_build_pairs: too many forests");
+  lya_resolve_build_timing(ctx);
+  cudaError_t e = nbr_reserve(ctx, n, nband);
   if (e != cudaSuccess) {
-    cleanup();
-    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_build_pairs: allocation failed");
+    lya_free_nbr_scratch(ctx->nbr);
+    return lya_fail(ctx, LYA_ERR_ALLOC, "lya_build_pairs: allocation of the search scratch failed (%s)",
+                    cudaGetErrorString(e));
   }
-  LYA_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
-  cudaMemsetAsync(flag, 0, sizeof(int), s);
-  cudaMemsetAsync(tot, 0, 2 * sizeof(double), s);
-  cudaMemsetAsync(counts, 0, sizeof(long long) * (n + 1), s);
+  NbrScratch& S = ctx->nbr;
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
-  k_bands<<<blocks, 256, 0, s>>>(n, ctx->cat.ra, ctx->cat.dec, h, nband, band, sra, sidx, flag);
-  ctx->launches++;
-  // order by (band, ra): stable sort by ra, then stable sort by band
-  thrust::stable_sort_by_key(pol, sra, sra + n, thrust::make_zip_iterator(thrust::make_tuple(sidx, band)));
-  thrust::stable_sort_by_key(pol, band, band + n, thrust::make_zip_iterator(thrust::make_tuple(sidx, sra)));
-  thrust::lower_bound(pol, band, band + n, thrust::counting_iterator<int32_t>(0),
-                      thrust::counting_iterator<int32_t>((int32_t)nband + 1), bstart);
-
+  const int nb_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nband + 1 + 127) / 128, 64));
   NbrParams p;
   p.n = n; p.ra = ctx->cat.ra; p.dec = ctx->cat.dec; p.ux = ctx->cat.ux; p.uy = ctx->cat.uy; p.uz = ctx->cat.uz;
-  p.name = ctx->cat.name; p.sidx = sidx; p.sra = sra; p.bstart = bstart; p.nband = nband; p.band_h = h;
-  p.angmax = angmax; p.mumin = mumin; p.ra_out_of_range = flag; p.counts = counts; p.offsets = offsets;
-  p.of1 = nullptr; p.of2 = nullptr;
+  p.name = ctx->cat.name; p.sidx = S.sidx; p.sra = S.sra; p.bstart = S.bstart; p.nband = nband; p.band_h = h;
+  p.angmax = angmax; p.mumin = mumin; p.ra_out_of_range = S.flag; p.len = ctx->cat.len; p.tot = S.tot;
+  p.counts = S.counts; p.offsets = S.offsets; p.of1 = nullptr; p.of2 = nullptr;
   const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, (int64_t)ctx->num_sms * 32));
-  k_neighbours<false><<<nblk, 256, 0, s>>>(p);
-  ctx->launches++;
-  thrust::exclusive_scan(pol, counts, counts + n + 1, offsets);
-  long long npairs = 0;
-  e = cudaMemcpyAsync(&npairs, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) {
-    cleanup();
-    return lya_fail(ctx, LYA_ERR_CUDA, "lya_build_pairs: %s", cudaGetErrorString(e));
+  size_t tb = S.tmp_bytes;
+  e = cudaEventRecord(S.ev0, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(S.flag, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(S.tot, 0, 2 * sizeof(double), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(S.counts, 0, sizeof(long long) * (n + 1), s);
+  if (e == cudaSuccess) {
+    k_bands<<<blocks, 256, 0, s>>>(n, ctx->cat.ra, S.sra2, S.sidx2, S.flag);
+    e = cudaGetLastError();
   }
+  // order by (band, ra): stable radix sort by ra, then stable radix sort by band
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairs(S.tmp, tb, S.sra2, S.sra, S.sidx2, S.sidx, (int)n, 0, 64, s);
+  if (e == cudaSuccess) {
+    k_band_keys<<<blocks, 256, 0, s>>>(n, S.sidx, ctx->cat.dec, h, nband, S.band2);
+    e = cudaGetLastError();
+  }
+  tb = S.tmp_bytes;
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairs(S.tmp, tb, S.band2, S.band, S.sidx, S.sidx2, (int)n, 0, 32, s);
+  if (e == cudaSuccess) {
+    std::swap(S.sidx, S.sidx2);   // sidx: forests in (band, ra) order
+    p.sidx = S.sidx;
+    k_gather_ra<<<blocks, 256, 0, s>>>(n, S.sidx, ctx->cat.ra, S.sra);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_band_starts<<<nb_blocks, 128, 0, s>>>(n, S.band, nband, S.bstart);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_neighbours<false><<<nblk, 256, 0, s>>>(p);
+    e = cudaGetLastError();
+  }
+  tb = S.tmp_bytes;
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(S.tmp, tb, S.counts, S.offsets, (int)(n + 1), s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(S.h_out, S.offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S.h_out + 1, S.tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // the one synchronisation: the queue's size
+  // k_bands, k_band_keys, k_gather_ra, k_band_starts, the count pass (the cub sorts and scan are library kernels)
+  ctx->launches += 5;
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_build_pairs: %s", cudaGetErrorString(e));
+  const long long npairs = S.h_out[0];
+  double ref[2];
+  memcpy(ref, S.h_out + 1, sizeof(ref));
   ctx->wq.n_pairs = 0;
   e = lya_queue_reserve(ctx->wq, npairs);
   if (e != cudaSuccess) {
-    cleanup();
     lya_free_queue(ctx->wq);
     return lya_fail(ctx, LYA_ERR_ALLOC, "lya_build_pairs: queue allocation failed (%lld pairs)", npairs);
   }
   p.of1 = ctx->wq.f1; p.of2 = ctx->wq.f2;
   k_neighbours<true><<<nblk, 256, 0, s>>>(p);
   ctx->launches++;
-  if (npairs > 0) {
-    const int cb = (int)std::min<int64_t>((npairs + 255) / 256, (int64_t)ctx->num_sms * 8);
-    k_pair_cost<<<cb, 256, 0, s>>>(npairs, ctx->wq.f1, ctx->wq.f2, ctx->cat.len, tot);
-    ctx->launches++;
-  }
-  double ref[2] = {0.0, 0.0};
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ref, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  float ms = 0.f;
-  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  cleanup();
+  if (e == cudaSuccess) e = cudaEventRecord(S.ev1, s);
   if (e != cudaSuccess) {
     lya_free_queue(ctx->wq);
     return lya_fail(ctx, LYA_ERR_CUDA, "lya_build_pairs: %s", cudaGetErrorString(e));
   }
+  S.timing_pending = true;   // build_ms is read once the fill pass has run (lya_stats)
   ctx->wq.n_pairs = npairs;
   ctx->wq.ref_pairs = ref[0];
   ctx->wq.ref_pixels = ref[1];
-  ctx->last.build_ms = ms;
   return LYA_OK;
 }
 
@@ -272,4 +387,72 @@ extern "C" int lya_build_pairs(lya_ctx* ctx, double angmax, double mumin, int64_
   const int rc = lya_build_queue(ctx, angmax, mumin);
   if (rc == LYA_OK && n_pairs_out) *n_pairs_out = ctx->wq.n_pairs;
   return rc;
+}
+
+extern "C" int lya_select_slots(lya_ctx* ctx, const uint8_t* keep) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_select_slots: ctx is NULL");
+  if (!keep) return lya_fail(ctx, LYA_ERR_ARG, "lya_select_slots: keep is NULL");
+  if (ctx->cat.n == 0) return lya_fail(ctx, LYA_ERR_STATE, "lya_select_slots: no forests uploaded");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  lya_resolve_build_timing(ctx);
+  ctx->have_result = false;
+  WorkQueue& q = ctx->wq;
+  const int64_t n = q.n_pairs;
+  const int32_t nslots = ctx->cat.n_slots;
+  SelectScratch& S = ctx->sel;
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  // scratch: keep flags per slot, per-item flags/positions, the compacted copy
+  if (!S.h_out) e = cudaMallocHost((void**)&S.h_out, sizeof(double) * 3);
+  if (e == cudaSuccess && !S.tot) e = lya_alloc(&S.tot, 2);
+  if (e == cudaSuccess && S.keep_cap < nslots) {
+    lya_free(S.keep);
+    S.keep_cap = 0;
+    e = lya_alloc(&S.keep, (size_t)std::max<int32_t>(nslots, 1));
+    if (e == cudaSuccess) S.keep_cap = nslots;
+  }
+  if (e == cudaSuccess && S.cap < std::max<int64_t>(n, 1)) {
+    lya_free(S.pos); lya_free(S.o1); lya_free(S.o2);
+    if (S.tmp) cudaFree(S.tmp);
+    S.tmp = nullptr; S.tmp_bytes = 0; S.cap = 0;
+    const int64_t c = std::max<int64_t>(n, 1);
+    e = lya_alloc(&S.pos, (size_t)c + 1);
+    if (e == cudaSuccess) e = lya_alloc(&S.o1, (size_t)c);
+    if (e == cudaSuccess) e = lya_alloc(&S.o2, (size_t)c);
+    size_t b = 0;
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, b, S.pos, S.pos, (int)(c + 1), s);
+    if (e == cudaSuccess) e = cudaMalloc(&S.tmp, std::max<size_t>(b, 16));
+    if (e == cudaSuccess) { S.tmp_bytes = std::max<size_t>(b, 16); S.cap = c; }
+  }
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "lya_select_slots: allocation failed (%s)",
+                                        cudaGetErrorString(e));
+  if (n >= (int64_t)INT32_MAX) return lya_fail(ctx, LYA_ERR_ARG, "lya_select_slots: queue too long");
+  e = cudaMemcpyAsync(S.keep, keep, (size_t)nslots, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(S.tot, 0, 2 * sizeof(double), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(S.pos + n, 0, sizeof(long long), s);
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+  if (e == cudaSuccess && n > 0) {
+    k_keep_flags<<<blocks, 256, 0, s>>>(n, q.f1, ctx->cat.slot, S.keep, S.pos);
+    e = cudaGetLastError();
+    size_t tb = S.tmp_bytes;
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(S.tmp, tb, S.pos, S.pos, (int)(n + 1), s);
+    if (e == cudaSuccess) {
+      k_keep_scatter<<<blocks, 256, 0, s>>>(n, q.f1, q.f2, S.keep, ctx->cat.slot, S.pos, ctx->cat.len, S.o1, S.o2,
+                                            S.tot);
+      e = cudaGetLastError();
+    }
+    ctx->launches += 2;
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S.h_out, S.pos + n, sizeof(long long), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S.h_out + 1, S.tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  long long kept = 0;
+  if (e == cudaSuccess) memcpy(&kept, S.h_out, sizeof(kept));
+  if (e == cudaSuccess && kept > 0) e = cudaMemcpyAsync(q.f1, S.o1, sizeof(int32_t) * kept, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && kept > 0) e = cudaMemcpyAsync(q.f2, S.o2, sizeof(int32_t) * kept, cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_select_slots: %s", cudaGetErrorString(e));
+  q.n_pairs = kept;
+  q.ref_pairs = S.h_out[1];
+  q.ref_pixels = S.h_out[2];
+  return LYA_OK;
 }

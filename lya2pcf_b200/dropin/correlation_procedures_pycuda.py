@@ -44,7 +44,8 @@ angmax = None
 _engine = None
 _slot_of_pixel = {}
 _computed = False
-_restrict = None
+_restrict = None            # owner slots of this rank's share (None: every pixel)
+_queue_restricted = False   # the device work queue holds only a share's pairs
 
 
 def _device():
@@ -61,7 +62,7 @@ def init(data_aux, log_file_aux, shape_hist_aux, angmax_aux, pixel_list=None):
     """Upload the forests of ``pixel_list`` (default: every pixel) and build the
     neighbour lists (``correlation_procedures_pycuda.py:16-111`` + the per-forest
     ``neighborhood`` calls of ``:144``)."""
-    global data, log_file, shape_hist, angmax, _engine, _slot_of_pixel, _computed, _restrict
+    global data, log_file, shape_hist, angmax, _engine, _slot_of_pixel, _computed, _restrict, _queue_restricted
     data = data_aux
     log_file = log_file_aux
     shape_hist = tuple(int(x) for x in shape_hist_aux)
@@ -77,32 +78,41 @@ def init(data_aux, log_file_aux, shape_hist_aux, angmax_aux, pixel_list=None):
     _slot_of_pixel = {int(p): s for s, p in enumerate(_engine.slot_pixels.tolist())}
     _computed = False
     _restrict = None
+    _queue_restricted = False
     if log_file is not None:
         log_file.write(f'\nUploaded {fs.n} forests ({fs.npix_total} pixels); {n_pairs} neighbouring forest pairs')
         log_file.flush()
 
 
 def restrict_pixels(pixels):
-    """Bin only the pairs owned by ``pixels`` (a contiguous run of the pixel
-    dict, e.g. one MPI rank's share) on the next computation."""
+    """Bin only the pairs owned by ``pixels`` (any subset of the pixel dict,
+    e.g. one rank's cost-balanced share) on the next computation."""
     global _restrict, _computed
-    slots = sorted(_slot_of_pixel[int(p)] for p in pixels if int(p) in _slot_of_pixel)
-    _restrict = (slots[0], slots[-1] + 1) if slots else (0, 0)
+    _restrict = frozenset(_slot_of_pixel[int(p)] for p in pixels if int(p) in _slot_of_pixel)
     _computed = False
 
 
 def _compute():
-    global _computed
+    global _computed, _queue_restricted
     if not _computed:
-        if _restrict != (0, 0):
-            _engine.run(kernel=KERNEL, guard=GUARD, slots=_restrict)
+        if _restrict is None:
+            if _queue_restricted:   # an earlier share compacted the queue: rebuild it
+                _engine.build_pairs(angmax)
+                _queue_restricted = False
+            _engine.run(kernel=KERNEL, guard=GUARD)
+        elif _restrict:
+            if _queue_restricted:
+                _engine.build_pairs(angmax)
+            _engine.select_slots(sorted(_restrict))
+            _queue_restricted = True
+            _engine.run(kernel=KERNEL, guard=GUARD)
         _computed = True
 
 
 def _slot_hist(pixel):
     _compute()
     s = _slot_of_pixel.get(int(pixel))
-    if s is None or (_restrict is not None and not (_restrict[0] <= s < _restrict[1])):
+    if s is None or (_restrict is not None and s not in _restrict):
         return None, None
     hist, cnt = _engine.histograms(s, 1)
     return hist[0], cnt[0]

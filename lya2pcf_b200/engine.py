@@ -133,6 +133,23 @@ class PairEngine:
         self._check(self.lib.lya_set_pairs(self.ctx, len(f1), N.ptr(f1), N.ptr(f2)))
         self.n_pairs = len(f1)
 
+    def select_slots(self, slots):
+        """Keep only the work-queue pairs whose first forest's owner slot is in
+        ``slots`` (an iterable of slot indices, or a boolean mask over the
+        slots): the rank-local queue of a sharded run.  Returns the pairs kept."""
+        n = len(self.slot_pixels)
+        keep = np.zeros(n, dtype=np.uint8)
+        slots = np.asarray(slots)
+        if slots.dtype == bool:
+            if slots.shape != (n,):
+                raise ValueError(f'slot mask must have {n} entries')
+            keep[slots] = 1
+        else:
+            keep[slots.astype(np.int64)] = 1
+        self._check(self.lib.lya_select_slots(self.ctx, N.ptr(keep)))
+        self.n_pairs = int(self.stats()['n_pairs'])
+        return self.n_pairs
+
     def get_pairs(self):
         f1 = np.zeros(max(self.n_pairs, 1), dtype=np.int32)
         f2 = np.zeros(max(self.n_pairs, 1), dtype=np.int32)

@@ -6,7 +6,10 @@ visible, gloo otherwise), else one process.
 The correlation needs no collective (owner pixels are disjoint; each rank
 writes its own files).  The distortion needs one: :meth:`Ranks.reduce_sum`
 adds the ranks' D (np*nt squared) and W_A to rank 0, which replaces
-``comm.reduce`` of ``distortion.py:118-119``.
+``comm.reduce`` of ``distortion.py:118-119``.  The adjoint over sharded owner
+pixels needs two: :meth:`Ranks.allreduce_sum` of the W and DW totals (to form
+xi on every rank) and of the per-pixel gradient vectors (a rank's pairs
+scatter into forests of any pixel).
 """
 import datetime
 import os
@@ -49,6 +52,24 @@ class Ranks:
                 t = t.cuda()
             dist.reduce(t, dst=0, op=dist.ReduceOp.SUM)
             out.append(t.cpu().numpy() if self.rank == 0 else a)
+        return tuple(out)
+
+    def allreduce_sum(self, *arrays):
+        """The element-wise sums of ``arrays`` over the ranks, on every rank
+        (float64 numpy arrays; the callers' arrays are not modified)."""
+        if self.size == 1:
+            return tuple(np.array(a, dtype=np.float64) for a in arrays)
+        if self.comm is not None:
+            return tuple(np.asarray(self.comm.allreduce(np.asarray(a, dtype=np.float64))) for a in arrays)
+        import torch
+        import torch.distributed as dist
+        out = []
+        for a in arrays:
+            t = torch.tensor(np.asarray(a, dtype=np.float64))
+            if self.cuda:
+                t = t.cuda()
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            out.append(t.cpu().numpy())
         return tuple(out)
 
     def close(self):

@@ -104,8 +104,8 @@ def _lognormal_positions(rng, n, ra_rng, dec_rng, corr_deg=2.0, sigma_ln=1.0, ce
     return ra, dec
 
 
-def _windows(rng, n, cfg):
-    lo, hi = cfg['length']
+def _windows(rng, n, cfg, length=None):
+    lo, hi = cfg['length'] if length is None else length
     length = rng.integers(lo, hi + 1, n)
     length = np.minimum(length, NGRID)
     if cfg['window'] == 'uniform':
@@ -132,8 +132,9 @@ def _project(w, delta, loglam):
     return dw, dl, sw, odl2
 
 
-def make(config, scale=1.0, seed=None, nside=16, n=None):
-    """Build the synthetic catalogue of benchmark configuration ``config``."""
+def make(config, scale=1.0, seed=None, nside=16, n=None, length=None):
+    """Build the synthetic catalogue of benchmark configuration ``config``;
+    ``length=(lo, hi)`` replaces the configuration's forest-length range."""
     cfg = CONFIGS[int(config)]
     rng = np.random.default_rng(SEEDS[int(config)] if seed is None else seed)
     n_forest = int(n) if n is not None else max(2, int(round(cfg['n'] * scale)))
@@ -153,7 +154,7 @@ def make(config, scale=1.0, seed=None, nside=16, n=None):
         ra[dst] = ra[src] + off
         dec[dst] = dec[src]
         name[dst] = name[src]
-    start_idx, length = _windows(rng, n_forest, cfg)
+    start_idx, length = _windows(rng, n_forest, cfg, length)
 
     grid_loglam = LOGLAM0 + DLOGLAM * np.arange(NGRID)
     grid_z = 10.0 ** grid_loglam / P.lambdaa - 1.0

@@ -38,6 +38,19 @@
  *                      compute_d) as distortion_procedures_pycuda.py:207-274
  *                      runs them per forest pair, in FP64 and with the FP64
  *                      binning of orc_corr.
+ *   orc_distortion_mode  the same sum with a choice of pair binning:
+ *                      ORC_BIN_FP64 (as orc_distortion) or ORC_BIN_FP32, the
+ *                      reference distortion's own FP32 binning of
+ *                      precompute_distances (cuda_kernels.cpp:67-84): FP32 dc and
+ *                      unit vectors, cos in FP32, the half-angle argument
+ *                      0.5*(1 +- cos) in FP64 rounded to FP32 for sqrtf,
+ *                      rp = |dc1-dc2|*ch and rt = (dc1+dc2)*sh in FP32, bins by
+ *                      truncation of rp*binner_rp and rt*binner_rt (FP32
+ *                      binners, parameters.py:14-21 via
+ *                      distortion_procedures_pycuda.py:167).
+ *   orc_dist_bins      the (bin_rp, bin_rt) of every pixel pair of one forest
+ *                      pair under either binning (the FP32 form is what
+ *                      precompute_distances writes).
  */
 #define _GNU_SOURCE
 #include <math.h>
@@ -49,6 +62,7 @@
 #define ORC_NQ 6 /* W, DW, RP, RT, Z, DWABS */
 
 enum { ORC_GPU_FORMULA = 0, ORC_CPU_FORMULA = 1 };
+enum { ORC_BIN_FP64 = 0, ORC_BIN_FP32 = 1 };
 
 /* cos of the pair angle as the reference GPU kernel computes it
  * (cuda_kernels.cpp:131, "x1*x2 + y1*y2 + z1*z2" in FP64).  nvcc contracts the
@@ -421,14 +435,95 @@ int orc_adjoint(const orc_forests* F, int64_t nitem, const int32_t* f1, const in
 }
 
 /* ------------------------------------------------------------ distortion */
+/* FP32 cos of the pair angle from FP32 unit vectors, in the contraction
+ * variants of orc_cos12 (cuda_kernels.cpp:72 is the same expression in float). */
+static float cos12_f32(float x1, float y1, float z1, float x2, float y2, float z2, int variant) {
+  switch (variant) {
+    case 0: return fmaf(z1, z2, fmaf(x1, x2, y1 * y2));
+    case 1: return fmaf(z1, z2, fmaf(y1, y2, x1 * x2));
+    default: {
+      float a = x1 * x2, b = y1 * y2, c = z1 * z2;
+      return (a + b) + c;
+    }
+  }
+}
+
+/* Pair geometry of one forest pair under a binning mode. */
+typedef struct {
+  int mode;
+  double chh, shh, brp, brt;     /* FP64 binning */
+  float ch32, sh32, brp32, brt32; /* FP32 binning */
+  int np, nt;
+} dist_geom;
+
+static void dist_geom_init(dist_geom* g, const orc_forests* F, int64_t a, int64_t b, double rpmax, double rtmax,
+                           int np, int nt, int cos_variant, int mode) {
+  g->mode = mode; g->np = np; g->nt = nt;
+  if (mode == ORC_BIN_FP32) {
+    float c = cos12_f32((float)F->ux[a], (float)F->uy[a], (float)F->uz[a], (float)F->ux[b], (float)F->uy[b],
+                        (float)F->uz[b], cos_variant);
+    /* cuda_kernels.cpp:73-74: the double literals 0.5 and 1. make the argument
+     * an FP64 value, rounded to FP32 by the sqrtf call */
+    g->ch32 = sqrtf((float)(0.5 * (1. + (double)c)));
+    g->sh32 = sqrtf((float)(0.5 * (1. - (double)c)));
+    /* distortion_procedures_pycuda.py:167: float32(numpix / rmax) */
+    g->brp32 = (float)((double)np / rpmax);
+    g->brt32 = (float)((double)nt / rtmax);
+  } else {
+    double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
+    g->chh = sqrt(0.5 * (1. + cos12));
+    g->shh = sqrt(0.5 * (1. - cos12));
+    g->brp = (double)np / rpmax;
+    g->brt = (double)nt / rtmax;
+  }
+}
+
+/* (bin_rp, bin_rt) of pixel pair (d1, d2); returns the flat bin or -1. */
+static int dist_bin(const dist_geom* g, double d1, double d2, int* bp_out, int* bt_out) {
+  if (g->mode == ORC_BIN_FP32) {
+    float f1 = (float)d1, f2 = (float)d2;
+    float rp = fabsf(f1 - f2) * g->ch32;
+    float rt = (f1 + f2) * g->sh32;
+    float xp = rp * g->brp32, xt = rt * g->brt32;
+    /* int() truncation; NaN and values beyond int range are reported as -1 */
+    int bp = (xp == xp && fabsf(xp) < 2.0e9f) ? (int)xp : -1;
+    int bt = (xt == xt && fabsf(xt) < 2.0e9f) ? (int)xt : -1;
+    if (bp_out) *bp_out = bp;
+    if (bt_out) *bt_out = bt;
+    if (bp < 0 || bt < 0 || bp >= g->np || bt >= g->nt) return -1;
+    return bp * g->nt + bt;
+  }
+  double fp = floor(fabs(d1 - d2) * g->chh * g->brp), ft = floor((d1 + d2) * g->shh * g->brt);
+  if (bp_out) *bp_out = (fp == fp && fabs(fp) < 2.0e9) ? (int)fp : -1;
+  if (bt_out) *bt_out = (ft == ft && fabs(ft) < 2.0e9) ? (int)ft : -1;
+  if (!(fp >= 0.0 && fp < (double)g->np && ft >= 0.0 && ft < (double)g->nt)) return -1;
+  return (int)fp * g->nt + (int)ft;
+}
+
+/* bin_rp[i*l2 + j], bin_rt[i*l2 + j] of forest pair (a, b). */
+int orc_dist_bins(const orc_forests* F, int32_t a, int32_t b, double rpmax, double rtmax, int np, int nt,
+                  int cos_variant, int bin_mode, int32_t* bin_rp, int32_t* bin_rt) {
+  dist_geom g;
+  dist_geom_init(&g, F, a, b, rpmax, rtmax, np, nt, cos_variant, bin_mode);
+  int64_t s1 = F->start[a], l1 = F->start[a + 1] - s1;
+  int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
+  for (int64_t i = 0; i < l1; ++i)
+    for (int64_t j = 0; j < l2; ++j) {
+      int bp, bt;
+      dist_bin(&g, F->dc[s1 + i], F->dc[s2 + j], &bp, &bt);
+      bin_rp[i * l2 + j] = bp;
+      bin_rt[i * l2 + j] = bt;
+    }
+  return 0;
+}
+
 /* Unnormalised distortion numerator D[A][B] and the bin weights W_B of the
  * listed forest pairs: the reference's compute_etas + compute_d per forest
- * pair (cuda_kernels.cpp:165-278) in FP64, pixel bins from the FP64 formula.
+ * pair (cuda_kernels.cpp:165-278) in FP64, pixel bins from the chosen binning.
  * D and WB are accumulated into.  Scratch is sized per forest pair here. */
-int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const int32_t* f2, double rpmax,
-                   double rtmax, int np, int nt, int cos_variant, double* D, double* WB) {
+int orc_distortion_mode(const orc_forests* F, int64_t nitem, const int32_t* f1, const int32_t* f2, double rpmax,
+                        double rtmax, int np, int nt, int cos_variant, int bin_mode, double* D, double* WB) {
   const int nb = np * nt;
-  const double binner_rp = (double)np / rpmax, binner_rt = (double)nt / rtmax;
   int64_t maxlen = 0;
   for (int64_t f = 0; f < F->n; ++f) if (F->start[f + 1] - F->start[f] > maxlen) maxlen = F->start[f + 1] - F->start[f];
   size_t big = (size_t)nb * (size_t)(maxlen > 0 ? maxlen : 1);
@@ -452,8 +547,8 @@ int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const
     int64_t a = f1[it], b = f2[it];
     int64_t s1 = F->start[a], l1 = F->start[a + 1] - s1;
     int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
-    double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], cos_variant);
-    double chh = sqrt(0.5 * (1. + cos12)), shh = sqrt(0.5 * (1. - cos12));
+    dist_geom g;
+    dist_geom_init(&g, F, a, b, rpmax, rtmax, np, nt, cos_variant, bin_mode);
     /* 1/sum(w) and 1/sum(w dl^2); a forest whose dl are all 0 (e.g. one pixel)
      * has no slope to project out, its slope terms are 0 instead of 0/0 */
     double om1 = F->omega[a], om2 = F->omega[b];
@@ -469,10 +564,7 @@ int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const
     for (int64_t i = 0; i < l1; ++i) {
       double d1 = F->dc[s1 + i], wi = F->w[s1 + i], li = F->dl[s1 + i];
       for (int64_t j = 0; j < l2; ++j) {
-        double d2 = F->dc[s2 + j];
-        double fp = floor(fabs(d1 - d2) * chh * binner_rp), ft = floor((d1 + d2) * shh * binner_rt);
-        int B = -1;
-        if (fp >= 0.0 && fp < (double)np && ft >= 0.0 && ft < (double)nt) B = (int)fp * nt + (int)ft;
+        int B = dist_bin(&g, d1, F->dc[s2 + j], 0, 0);
         bins[i * l2 + j] = B;
         if (B < 0) continue;
         double wj = F->w[s2 + j], lj = F->dl[s2 + j];
@@ -512,4 +604,9 @@ int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const
   free(e12); free(e21); free(e13); free(e31); free(e22); free(e23); free(e32); free(e33);
   free(act); free(actlist); free(bins);
   return 0;
+}
+
+int orc_distortion(const orc_forests* F, int64_t nitem, const int32_t* f1, const int32_t* f2, double rpmax,
+                   double rtmax, int np, int nt, int cos_variant, double* D, double* WB) {
+  return orc_distortion_mode(F, nitem, f1, f2, rpmax, rtmax, np, nt, cos_variant, ORC_BIN_FP64, D, WB);
 }

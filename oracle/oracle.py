@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, '_build', 'liboracle.so')
 NQ = 6
 Q_W, Q_DW, Q_RP, Q_RT, Q_Z, Q_DWABS = range(NQ)
 GPU_FORMULA, CPU_FORMULA = 0, 1
+BIN_FP64, BIN_FP32 = 0, 1
 
 _lib = None
 
@@ -43,9 +44,14 @@ def lib():
                                C.c_double, P, P, C.c_int]
         L.orc_adjoint.argtypes = [P, C.c_int64, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, P, P, P, P]
         L.orc_distortion.argtypes = [P, C.c_int64, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, P, P]
+        L.orc_distortion_mode.argtypes = [P, C.c_int64, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, P, P]
+        L.orc_dist_bins.argtypes = [P, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, P, P]
         L.orc_cos12.argtypes = [C.c_double] * 6 + [C.c_int]
         L.orc_cos12.restype = C.c_double
-        for f in ('orc_neighbours', 'orc_corr', 'orc_adjoint', 'orc_distortion'):
+        for f in ('orc_neighbours', 'orc_corr', 'orc_adjoint', 'orc_distortion', 'orc_distortion_mode',
+                  'orc_dist_bins'):
             getattr(L, f).restype = C.c_int
         _lib = L
     return _lib
@@ -162,18 +168,33 @@ def adjoint(fs, f1, f2, coef_dw, coef_w, rpmax=200.0, rtmax=200.0, np_=50, nt=50
     return g_dw, g_w
 
 
-def distortion(fs, f1, f2, rpmax=200.0, rtmax=200.0, np_=50, nt=50, cos_variant=0, cat=None):
-    """Unnormalised distortion numerator D[nb, nb] and bin weights W_B[nb]."""
+def distortion(fs, f1, f2, rpmax=200.0, rtmax=200.0, np_=50, nt=50, cos_variant=0, bin_mode=BIN_FP64, cat=None):
+    """Unnormalised distortion numerator D[nb, nb] and bin weights W_B[nb].
+    ``bin_mode`` BIN_FP64 bins pairs with the correlation's FP64 formula,
+    BIN_FP32 with the reference distortion's FP32 precompute_distances."""
     cat = cat or Catalog(fs)
     nb = np_ * nt
     D = np.zeros((nb, nb), dtype=np.float64)
     WB = np.zeros(nb, dtype=np.float64)
     f1 = np.ascontiguousarray(f1, dtype=np.int32)
     f2 = np.ascontiguousarray(f2, dtype=np.int32)
-    rc = lib().orc_distortion(cat.ref, len(f1), _ptr(f1), _ptr(f2), float(rpmax), float(rtmax), int(np_), int(nt),
-                              int(cos_variant), _ptr(D), _ptr(WB))
+    rc = lib().orc_distortion_mode(cat.ref, len(f1), _ptr(f1), _ptr(f2), float(rpmax), float(rtmax), int(np_),
+                                   int(nt), int(cos_variant), int(bin_mode), _ptr(D), _ptr(WB))
     assert rc == 0
     return D, WB
+
+
+def dist_bins(fs, a, b, rpmax=200.0, rtmax=200.0, np_=50, nt=50, cos_variant=0, bin_mode=BIN_FP32, cat=None):
+    """(bin_rp, bin_rt) int32 [len_a, len_b] of forest pair (a, b)."""
+    cat = cat or Catalog(fs)
+    la, lb = int(fs.start[a + 1] - fs.start[a]), int(fs.start[b + 1] - fs.start[b])
+    bp = np.zeros((la, lb), dtype=np.int32)
+    bt = np.zeros((la, lb), dtype=np.int32)
+    if la and lb:
+        rc = lib().orc_dist_bins(cat.ref, int(a), int(b), float(rpmax), float(rtmax), int(np_), int(nt),
+                                 int(cos_variant), int(bin_mode), _ptr(bp), _ptr(bt))
+        assert rc == 0
+    return bp, bt
 
 
 def pair_count_total(fs, f1, f2):

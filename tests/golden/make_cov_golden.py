@@ -1,7 +1,7 @@
 """Golden vectors of the reference's covariance post-processing.
 
-Run where the lya2pcf reference tree is available (LYA2PCF_REFERENCE, default
-/root/reference).  ``post_processing.py`` imports fitsio at module level,
+Run where the lya2pcf reference tree is available, named by the required
+LYA2PCF_REFERENCE environment variable.  ``post_processing.py`` imports fitsio at module level,
 which is not installed here, so the script compiles only the definitions of
 ``bin_coordinates``, ``cov`` (numba), ``cov_smooth`` and ``diag_error``
 (post_processing.py:13-109) taken verbatim from that file's syntax tree, runs
@@ -21,7 +21,9 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get('LYA2PCF_REFERENCE', '/root/reference')
+REF = os.environ.get('LYA2PCF_REFERENCE', '')
+if __name__ == '__main__' and not REF:
+    raise SystemExit('set LYA2PCF_REFERENCE to the lya2pcf reference tree')
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -1,8 +1,8 @@
 """Golden vectors of the reference's delta projection, quasar.fill_dw
 (forest_class.py:48-68).
 
-Run where the lya2pcf reference tree is available (LYA2PCF_REFERENCE, default
-/root/reference).  ``forest_class.py`` imports healpy at module level, which is
+Run where the lya2pcf reference tree is available, named by the required
+LYA2PCF_REFERENCE environment variable.  ``forest_class.py`` imports healpy at module level, which is
 not installed here, so the script compiles only the ``fill_dw`` method of the
 ``quasar`` class from that file's syntax tree and calls it on a stand-in
 object holding the weights.  Writes ``tests/golden/fill_dw_golden.npz``:
@@ -17,7 +17,9 @@ import types
 
 import numpy as np
 
-REF = os.environ.get('LYA2PCF_REFERENCE', '/root/reference')
+REF = os.environ.get('LYA2PCF_REFERENCE', '')
+if __name__ == '__main__' and not REF:
+    raise SystemExit('set LYA2PCF_REFERENCE to the lya2pcf reference tree')
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

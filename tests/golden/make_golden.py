@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
-Runs in a container where the lya2pcf reference tree is mounted (default
-``/root/reference``, override with ``LYA2PCF_REFERENCE``): it imports the
+Runs where the lya2pcf reference tree is available, named by the required
+``LYA2PCF_REFERENCE`` environment variable: it imports the
 reference's numba CPU kernel ``correlation_procedures_cpu.pair_correlation``
 (``correlation_procedures_cpu.py:46-84``) and its ``two_point_per_pixel`` driver
 (``:19-43``), feeds them seeded synthetic forests, and stores inputs and outputs
@@ -9,14 +9,16 @@ as ``.npz`` (``numba_pairs``: hand-placed pairs; ``numba_sweep``: seeded random
 pairs over the whole sky; ``numba_pixel``: one pixel through the driver).  The GPU test machine has no reference tree; it only reads the
 committed ``.npz`` files.
 
-    python tests/golden/make_golden.py
+    LYA2PCF_REFERENCE=<reference tree> python tests/golden/make_golden.py
 """
 import os
 import sys
 
 import numpy as np
 
-REF = os.environ.get('LYA2PCF_REFERENCE', '/root/reference')
+REF = os.environ.get('LYA2PCF_REFERENCE', '')
+if __name__ == '__main__' and not REF:
+    raise SystemExit('set LYA2PCF_REFERENCE to the lya2pcf reference tree')
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

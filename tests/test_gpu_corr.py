@@ -58,13 +58,23 @@ def test_device_neighbours_equal_oracle(cfg0):
     assert st['ref_pairs'] == float(np.sum(fs.lengths[o1] * fs.lengths[nbr]))
 
 
-@pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
-def test_config0_slots_match_oracle(cfg0, kern, var):
+@pytest.fixture(scope='module')
+def cfg0_oracle(cfg0):
+    """The oracle's histograms of every owner slot of the small configuration
+    (7e10 pixel pairs, all host threads)."""
     fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
-    ns = 4
-    ho, co = O.corr(fs, f1[:sis[ns]], f2[:sis[ns]], sis[:ns + 1])
+    return O.corr(fs, f1, f2, sis)
+
+
+@pytest.mark.parametrize('kern,var', CASES, ids=CASE_IDS)
+def test_config0_all_slots_match_oracle(cfg0, cfg0_oracle, kern, var):
+    """Every owner slot of the small configuration: counts bit-exact against
+    the oracle, sums within the kernel's tolerance."""
+    fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
+    ho, co = cfg0_oracle
+    assert len(pixels) >= 30
     eng.run(kernel=kern, variant=var)
-    h, c = eng.histograms(0, ns)
+    h, c = eng.histograms()
     check_hist(h, c, ho, co, kern, f'kernel {kern}')
 
 
@@ -260,3 +270,20 @@ def test_autotune_choice_keeps_parity(cfg0):
     h, c = eng.histograms(0, ns)
     check_hist(h, c, ho, co, N.KERNEL_FP32_GUARDED, 'autotuned')
     eng.tuned.clear()
+
+
+def test_device_neighbours_equal_reference_neighborhood():
+    """The device work queue equals the reference's own quasar.neighborhood
+    lists (golden vectors, tests/golden/make_neighbour_golden.py) as sets per
+    first forest."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'neighbour_golden.npz'))
+    for fs, tag in ((synthetic.make(0, n=400), 'cat0'), (E.edge_catalog(), 'edge')):
+        off, nbr = g[f'{tag}_off'], g[f'{tag}_nbr']
+        with PairEngine() as eng:
+            eng.upload(fs)
+            n = eng.build_pairs(float(g[f'{tag}_angmax']))
+            d1, d2 = eng.get_pairs()
+        assert n == len(nbr) > 0
+        for f in range(fs.n):
+            assert sorted(d2[d1 == f].tolist()) == sorted(nbr[off[f]:off[f + 1]].tolist()), (tag, f)

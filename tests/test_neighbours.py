@@ -52,3 +52,21 @@ def test_dropin_neighborhood_same_as_oracle():
     for k, q in enumerate(flat):
         got = [index[id(o)] for o in q.neighborhood(data, am)]
         assert got == nbr[off[k]:off[k + 1]].tolist(), k
+
+
+def _golden_neighbours():
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'neighbour_golden.npz'))
+    return [(synthetic.make(0, n=400), 'cat0', g), (E.edge_catalog(), 'edge', g)]
+
+
+def test_oracle_neighbours_equal_reference_neighborhood():
+    """The oracle's neighbour lists equal the reference's own
+    quasar.neighborhood (forest_class.py:78-98, run under a healpy stand-in
+    whose query_disc returns every pixel: tests/golden/make_neighbour_golden.py),
+    forest by forest, in the same order."""
+    for fs, tag, g in _golden_neighbours():
+        assert int(g[f'{tag}_n']) == fs.n
+        off, nbr = O.neighbours(fs, float(g[f'{tag}_angmax']))
+        assert np.array_equal(off, g[f'{tag}_off']), tag
+        assert np.array_equal(nbr, g[f'{tag}_nbr']), tag

@@ -209,3 +209,48 @@ def test_distortion_matches_eta_product_form():
     De, WBe = _eta_form_distortion(fs, f1, f2)
     np.testing.assert_allclose(WB, WBe, rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(D, De, rtol=1e-9, atol=1e-9 * np.abs(De).max())
+
+
+def test_fp32_distortion_binning_matches_numpy_float32():
+    """The oracle's FP32 binning (the reference distortion's
+    precompute_distances, cuda_kernels.cpp:67-84) in its uncontracted variant
+    against the same arithmetic in numpy float32: FP32 unit vectors and dc,
+    the half-angle argument 0.5*(1 +- cos) in FP64 rounded to FP32 before
+    sqrtf, FP32 products, truncation of rp*binner and rt*binner."""
+    from lya2pcf_b200 import synthetic
+    fs = synthetic.make(4, n=12, length=(20, 60))
+    f32 = np.float32
+    for a, b in ((0, 1), (2, 5), (3, 11), (7, 4)):
+        bp, bt = O.dist_bins(fs, a, b, cos_variant=2, bin_mode=O.BIN_FP32)
+        u1 = [f32(fs.ux[a]), f32(fs.uy[a]), f32(fs.uz[a])]
+        u2 = [f32(fs.ux[b]), f32(fs.uy[b]), f32(fs.uz[b])]
+        c = (u1[0] * u2[0] + u1[1] * u2[1]) + u1[2] * u2[2]
+        ch = np.sqrt(f32(0.5 * (1.0 + np.float64(c))))
+        sh = np.sqrt(f32(0.5 * (1.0 - np.float64(c))))
+        d1 = fs.dc[fs.start[a]:fs.start[a + 1]].astype(f32)
+        d2 = fs.dc[fs.start[b]:fs.start[b + 1]].astype(f32)
+        rp = np.abs(d1[:, None] - d2[None, :]) * ch
+        rt = (d1[:, None] + d2[None, :]) * sh
+        assert rp.dtype == f32 and rt.dtype == f32
+        assert np.array_equal(bp, (rp * f32(0.25)).astype(np.int32))
+        assert np.array_equal(bt, (rt * f32(0.25)).astype(np.int32))
+        # the FP64 binning of the same pair is a different function
+        b64p, b64t = O.dist_bins(fs, a, b, bin_mode=O.BIN_FP64)
+        assert np.array_equal(b64p, np.floor(np.abs(fs.dc[fs.start[a]:fs.start[a + 1], None]
+                                                    - fs.dc[None, fs.start[b]:fs.start[b + 1]])
+                                             * np.sqrt(0.5 * (1.0 + O.cos12((fs.ux[a], fs.uy[a], fs.uz[a]),
+                                                                            (fs.ux[b], fs.uy[b], fs.uz[b]), 0)))
+                                             * 0.25).astype(np.int32))
+
+
+def test_distortion_fp32_binning_differs_only_through_bins():
+    """With the FP32 binning the oracle's W_B differs from the FP64 binning's
+    (some pairs change bins) while its total stays within 1%."""
+    from lya2pcf_b200 import synthetic
+    fs = synthetic.make(4, n=14, length=(20, 80))
+    off, nbr = O.neighbours(fs, synthetic.angmax_for(fs))
+    f1, f2, _, _ = O.items_from_csr(fs, off, nbr)
+    D64, W64 = O.distortion(fs, f1, f2, bin_mode=O.BIN_FP64)
+    D32, W32 = O.distortion(fs, f1, f2, bin_mode=O.BIN_FP32)
+    assert W64.sum() > 0 and not np.array_equal(W32, W64)
+    np.testing.assert_allclose(W32.sum(), W64.sum(), rtol=1e-2)
