@@ -48,6 +48,7 @@ UNIT = 'pixel-pairs/s'
 WORKLOAD = ('150,000 synthetic Lyman-alpha forests on 8,000 deg^2 (19/deg^2), lengths U[50,700] clamped to the '
             '614-pixel log-lambda grid, 50x50 (r_par, r_perp) bins to 200 Mpc/h, float64 inputs')
 GUARD = 1e-4     # Mpc/h guard band of the FP32 kernel
+DMMA_PEAK_TFLOPS = 40.0   # B200 FP64 tensor-core rate, data sheet (the distortion's block products)
 KERNEL_CODES = {'fp32': 0, 'fp64diag': 1, 'fp64plain': 2}
 
 
@@ -490,12 +491,21 @@ def distortion_sample(scale, dev):
         f1, f2 = eng.get_pairs()
         L = fs.lengths.astype(np.float64)
         ref = float(np.sum(L[f1] * L[f2]))
+        tune = eng.autotune_distortion()
         eng.distortion()
         D, W = eng.distortion()
-        ms = eng.stats()['kernel_ms']
+        st = eng.stats()
+        ms = st['kernel_ms']
+    flops = st['dist_mma_flops']
     return {'forests': fs.n, 'scale': scale, 'forest_pairs': n, 'ref_pixel_pairs': ref, 'kernel_ms': ms,
             'forest_pairs_per_s': n / (ms * 1e-3), 'ref_pixel_pairs_per_s': ref / (ms * 1e-3),
-            'matrix': f'{D.shape[0]}x{D.shape[1]} float64, {int(np.count_nonzero(D))} nonzero'}
+            'matrix': f'{D.shape[0]}x{D.shape[1]} float64, {int(np.count_nonzero(D))} nonzero',
+            'tuned': tune,
+            'roofline': {'bound': 'fp64_tensor', 'achieved': flops / (ms * 1e-3) / 1e12, 'unit': 'TFLOP/s',
+                         'peak': DMMA_PEAK_TFLOPS, 'frac': flops / (ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS,
+                         'flops': flops,
+                         'peak_source': 'nominal B200 FP64 tensor-core rate (data sheet, not measured)',
+                         'what': 'm8n8k4 FP64 MMAs of the column block products (counted by the kernel)'}}
 
 
 XI_FLOOR_FRAC = 0.1   # per-bin xi errors are stated over bins with |xi| >= this fraction of the median |xi|
@@ -675,9 +685,14 @@ def profile_case(args):
         eng.upload(fs)
         eng.build_pairs(synthetic.angmax_for(fs))
         if args.profile_case == 'dist':
+            tune = eng.autotune_distortion()
             eng.distortion()
+            t = time.perf_counter()
             eng.distortion()
             st = eng.stats()
+            st['dist_wall_s'] = time.perf_counter() - t
+            st['tuned'] = tune
+            st['forest_pairs'] = eng.n_pairs
         elif args.profile_case == 'adjoint':
             eng.run(kernel=kern, guard=GUARD)
             g = np.random.default_rng(4).normal(size=eng.nb)

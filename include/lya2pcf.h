@@ -74,6 +74,8 @@ typedef struct {
   double run_ref_pairs;    /* reference pair count of the last run's slot range */
   int64_t launches;        /* kernels of this library launched by the context so far */
   double ref_pixels;       /* sum over forest pairs of len1+len2 */
+  double adjoint_ms;       /* device time of the last lya_corr_adjoint's gradient kernels */
+  double dist_mma_flops;   /* FP64 tensor-core flops of the last lya_dist_run (block products) */
 } lya_stats_t;
 
 /* ----------------------------------------------------------------- context */
@@ -157,10 +159,18 @@ int lya_corr_get(lya_ctx* ctx, int32_t slot_first, int32_t n, double* hist, uint
 
 /* Gradient of L = sum_b g[b] * DW_b / W_b (totals over all slots of the last
  * lya_corr_run) with the pair bins held fixed: grad_dw and grad_w per pixel of
- * the catalogue (CSR order).  g is a host array of np*nt values; grad_dw and
- * grad_w are host arrays, or device arrays on the context's device when
- * device_ptrs is 1.  No reference counterpart. */
+ * the catalogue (CSR order).  g has np*nt values; device_ptrs bit 0: grad_dw
+ * and grad_w are device arrays on the context's device (else host arrays);
+ * bit 1: g is a device array (else a host array).  lya_stats' adjoint_ms is
+ * the device time of the gradient kernels.  No reference counterpart. */
 int lya_corr_adjoint(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int32_t device_ptrs);
+
+/* Totals over all owner slots of the last lya_corr_run: W[b] = sum w1w2 and
+ * DW[b] = sum dw1dw2 (np*nt values each; host arrays, or device arrays when
+ * device_ptrs is 1).  The sums post_processing.py:134-149 forms from the
+ * per-pixel files; used for xi = DW/W without copying every pixel's
+ * histograms.  No reference counterpart. */
+int lya_corr_totals(lya_ctx* ctx, double* W, double* DW, int32_t device_ptrs);
 
 /* Replace the weights w and weighted deltas dw of every pixel (CSR order, as
  * uploaded) without re-uploading the catalogue; host arrays, or device arrays
@@ -176,8 +186,15 @@ int lya_update_weights(lya_ctx* ctx, const double* w, const double* dw, int32_t 
  * precompute_distances, compute_etas, order_active, compute_d
  * (cuda_kernels.cpp:46-87, 165-278).  The normalised matrix of distortion.py:125
  * is D / W[:, None].  Needs dl, omega and odl2 at upload; a pixel whose
- * partners fall in more than 6 rt bins is reported as LYA_ERR_DATA. */
+ * partners fall in more than 8 rt bins is reported as LYA_ERR_DATA. */
 int lya_dist_run(lya_ctx* ctx, double* D, double* W);
+
+/* Launch shape of lya_dist_run's kernel (0 = default: 512 threads per CTA,
+ * rows staged 32 pixels at a time; 1..4 = 512/16, 512/64, 256/32, 256/16) and
+ * an optional limit: max_items > 0 bins only the first max_items forest pairs
+ * of the work queue (a timing sample for the autotuner), 0 = all.  Stays in
+ * effect for later calls.  No reference counterpart. */
+int lya_dist_config(lya_ctx* ctx, int32_t shape, int64_t max_items);
 
 int lya_stats(lya_ctx* ctx, lya_stats_t* out);
 

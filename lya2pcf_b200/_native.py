@@ -43,9 +43,11 @@ SIGNATURES = {
     'lya_corr_get': ([P, C.c_int32, C.c_int32, P, P], C.c_int),
     'lya_corr_adjoint': ([P, P, P, P, C.c_int32], C.c_int),
     'lya_update_weights': ([P, P, P, C.c_int32], C.c_int),
+    'lya_corr_totals': ([P, P, P, C.c_int32], C.c_int),
     'lya_stats': ([P, P], C.c_int),
     'lya_timer': ([P, C.c_int32, C.POINTER(C.c_double)], C.c_int),
     'lya_dist_run': ([P, P, P], C.c_int),
+    'lya_dist_config': ([P, C.c_int32, C.c_int64], C.c_int),
     'lya_sync': ([P], C.c_int),
     'lya_covariance': ([P, C.c_int64, P, P, P, P], C.c_int),
     'lya_covariance_smooth': ([P, P, P, C.POINTER(C.c_int32)], C.c_int),
@@ -71,7 +73,8 @@ class Stats(C.Structure):
                 ('runs_flushed', C.c_double), ('in_range_pairs', C.c_double), ('kernel_ms', C.c_double),
                 ('build_ms', C.c_double), ('n_pairs', C.c_int64), ('n_slots', C.c_int32), ('n_forests', C.c_int32),
                 ('guard_bound', C.c_double), ('run_ms', C.c_double), ('run_ref_pairs', C.c_double),
-                ('launches', C.c_int64), ('ref_pixels', C.c_double)]
+                ('launches', C.c_int64), ('ref_pixels', C.c_double), ('adjoint_ms', C.c_double),
+                ('dist_mma_flops', C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

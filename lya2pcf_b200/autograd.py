@@ -19,6 +19,12 @@ from . import _native as N
 
 
 class _Xi(torch.autograd.Function):
+    """Forward: the library's histograms of the given (w, dw), reduced to the
+    totals W, DW on the device (lya_corr_totals) and xi = DW/W in torch.
+    Backward: lya_corr_adjoint with g on the device and the gradients written
+    into device tensors.  Only the library's stream and torch's current stream
+    are synchronised between the two (no host copies of histograms)."""
+
     @staticmethod
     def forward(ctx, w, dw, engine, kernel):
         if not (w.is_cuda and dw.is_cuda):
@@ -28,21 +34,22 @@ class _Xi(torch.autograd.Function):
         torch.cuda.current_stream(w.device).synchronize()
         engine.update_weights(w64, dw64)
         engine.run(kernel=kernel)
-        hist, _ = engine.histograms()
-        W = hist[:, N.Q_W].sum(0)
-        DW = hist[:, N.Q_DW].sum(0)
-        xi = np.divide(DW, W, out=np.zeros_like(W), where=W != 0)
+        W = torch.empty(engine.nb, dtype=torch.float64, device=w.device)
+        DW = torch.empty_like(W)
+        engine.totals(out_w=W, out_dw=DW)
+        xi_ = torch.where(W != 0, DW / torch.where(W != 0, W, torch.ones_like(W)), torch.zeros_like(W))
         ctx.engine = engine
         ctx.shape = w64.shape
         ctx.device = w.device
         ctx.dtypes = (w.dtype, dw.dtype)
-        return torch.from_numpy(xi).to(device=w.device, dtype=w.dtype)
+        return xi_.to(dtype=w.dtype)
 
     @staticmethod
     def backward(ctx, gxi):
-        g = gxi.detach().to(torch.float64).cpu().numpy()
+        g = gxi.detach().to(torch.float64).contiguous()
         gdw = torch.empty(ctx.shape, dtype=torch.float64, device=ctx.device)
         gw = torch.empty(ctx.shape, dtype=torch.float64, device=ctx.device)
+        torch.cuda.current_stream(ctx.device).synchronize()
         ctx.engine.adjoint(g, out_dw=gdw, out_w=gw)
         return gw.to(ctx.dtypes[0]), gdw.to(ctx.dtypes[1]), None, None
 

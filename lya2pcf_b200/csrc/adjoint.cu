@@ -60,6 +60,21 @@ __global__ void k_coef(int nslots, int nb, const double* __restrict__ hist, cons
   }
 }
 
+// Totals over all slots of the last run: W[b] and DW[b] (hi + lo of each slot).
+__global__ void k_totals(int nslots, int nb, const double* __restrict__ hist, double* __restrict__ W,
+                         double* __restrict__ DW) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    double w = 0.0, dw = 0.0;
+    for (int s = 0; s < nslots; ++s) {
+      const double* h = hist + (size_t)s * LYA_NQ * 2 * nb;
+      w += h[(0 * 2 + 0) * nb + b] + h[(0 * 2 + 1) * nb + b];
+      dw += h[(1 * 2 + 0) * nb + b] + h[(1 * 2 + 1) * nb + b];
+    }
+    W[b] = w;
+    DW[b] = dw;
+  }
+}
+
 // Reversed-direction flag is in the item index: items [0, n) are (f1, f2),
 // items [n, 2n) are (f2, f1).
 __global__ void __launch_bounds__(256) k_adjoint(const AdjParams p) {
@@ -133,25 +148,43 @@ __global__ void k_unpad(int64_t n, const int64_t* __restrict__ start, const int6
 
 }  // namespace
 
+// Scratch of the adjoint, kept in the context between calls (grown, never shrunk).
+static cudaError_t adjoint_reserve(lya_ctx* ctx, int nb, int64_t n, int64_t npad, int64_t npix) {
+  AdjScratch& S = ctx->adj;
+  if (S.g && S.nb >= nb && S.n >= n && S.npad >= npad && S.npix >= npix) return cudaSuccess;
+  lya_free(S.g); lya_free(S.coef); lya_free(S.gdw); lya_free(S.gw); lya_free(S.out); lya_free(S.start);
+  S = AdjScratch{};
+  cudaError_t e = lya_alloc(&S.g, nb);
+  if (e == cudaSuccess) e = lya_alloc(&S.coef, 2 * (size_t)nb);
+  if (e == cudaSuccess) e = lya_alloc(&S.gdw, npad);
+  if (e == cudaSuccess) e = lya_alloc(&S.gw, npad);
+  if (e == cudaSuccess) e = lya_alloc(&S.out, npix);
+  if (e == cudaSuccess) e = lya_alloc(&S.start, n + 1);
+  if (e != cudaSuccess) {
+    lya_free(S.g); lya_free(S.coef); lya_free(S.gdw); lya_free(S.gw); lya_free(S.out); lya_free(S.start);
+    S = AdjScratch{};
+    return e;
+  }
+  S.nb = nb; S.n = n; S.npad = npad; S.npix = npix;
+  return cudaSuccess;
+}
+
 int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* grad_w, int device_ptrs) {
   const int nb = ctx->np * ctx->nt;
   const int64_t n = ctx->cat.n;
   const int64_t npad = ctx->cat.npad, npix = ctx->cat.npix;
   cudaStream_t s = ctx->stream;
-  double *d_g = nullptr, *coef = nullptr, *gdw = nullptr, *gw = nullptr, *out = nullptr;
-  int64_t* d_start = nullptr;
-  cudaError_t e = lya_alloc(&d_g, nb);
-  if (e == cudaSuccess) e = lya_alloc(&coef, 2 * nb);
-  if (e == cudaSuccess) e = lya_alloc(&gdw, npad);
-  if (e == cudaSuccess) e = lya_alloc(&gw, npad);
-  if (e == cudaSuccess) e = lya_alloc(&out, npix);
-  if (e == cudaSuccess) e = lya_alloc(&d_start, n + 1);
-  auto cleanup = [&]() { lya_free(d_g); lya_free(coef); lya_free(gdw); lya_free(gw); lya_free(out); lya_free(d_start); };
-  if (e != cudaSuccess) { cleanup(); return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_adjoint: allocation failed"); }
-  e = cudaMemcpyAsync(d_g, g, sizeof(double) * nb, cudaMemcpyHostToDevice, s);
+  cudaError_t e = adjoint_reserve(ctx, nb, n, npad, npix);
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_adjoint: allocation failed");
+  AdjScratch& S = ctx->adj;
+  double *d_g = S.g, *coef = S.coef, *gdw = S.gdw, *gw = S.gw, *out = S.out;
+  int64_t* d_start = S.start;
+  e = cudaMemcpyAsync(d_g, g, sizeof(double) * nb, (device_ptrs & 2) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                      s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_start, ctx->h_start.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(gdw, 0, sizeof(double) * npad, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(gw, 0, sizeof(double) * npad, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, s);
   if (e == cudaSuccess) {
     k_coef<<<(nb + 255) / 256, 256, 0, s>>>(ctx->hist_slots, nb, ctx->hist, d_g, coef);
     ctx->launches++;
@@ -170,9 +203,10 @@ int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* g
     }
     if (e == cudaSuccess) e = cudaGetLastError();
   }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
   if (e == cudaSuccess && n > 0) {
     const int blocks = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
-    if (device_ptrs) {
+    if (device_ptrs & 1) {
       if (grad_dw) { k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gdw, grad_dw); ctx->launches++; }
       if (grad_w) { k_unpad<<<blocks, 128, 0, s>>>(n, d_start, ctx->cat.pstart, gw, grad_w); ctx->launches++; }
     } else {
@@ -186,8 +220,36 @@ int lya_adjoint_launch(lya_ctx* ctx, const double* g, double* grad_dw, double* g
     }
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cleanup();
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_corr_adjoint: %s", cudaGetErrorString(e));
+  ctx->last.adjoint_ms = ms;
+  return LYA_OK;
+}
+
+extern "C" int lya_corr_totals(lya_ctx* ctx, double* W, double* DW, int32_t device_ptrs) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_corr_totals: ctx is NULL");
+  if (!W || !DW) return lya_fail(ctx, LYA_ERR_ARG, "lya_corr_totals: NULL output");
+  if (!ctx->have_result) return lya_fail(ctx, LYA_ERR_STATE, "lya_corr_totals: run lya_corr_run first");
+  LYA_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nb = ctx->np * ctx->nt;
+  cudaStream_t s = ctx->stream;
+  if (device_ptrs) {
+    k_totals<<<(nb + 255) / 256, 256, 0, s>>>(ctx->hist_slots, nb, ctx->hist, W, DW);
+    ctx->launches++;
+    LYA_CHECK_CUDA(ctx, cudaGetLastError());
+    LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    return LYA_OK;
+  }
+  cudaError_t e = adjoint_reserve(ctx, nb, ctx->cat.n, ctx->cat.npad, ctx->cat.npix);
+  if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_ALLOC, "lya_corr_totals: allocation failed");
+  double* t = ctx->adj.coef;   // [2][nb]
+  k_totals<<<(nb + 255) / 256, 256, 0, s>>>(ctx->hist_slots, nb, ctx->hist, t, t + nb);
+  ctx->launches++;
+  LYA_CHECK_CUDA(ctx, cudaGetLastError());
+  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(W, t, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+  LYA_CHECK_CUDA(ctx, cudaMemcpyAsync(DW, t + nb, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+  LYA_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   return LYA_OK;
 }
 

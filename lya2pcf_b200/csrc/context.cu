@@ -199,6 +199,8 @@ extern "C" int lya_ctx_destroy(lya_ctx* ctx) {
   if (ctx->sel.tmp) cudaFree(ctx->sel.tmp);
   if (ctx->sel.h_out) cudaFreeHost(ctx->sel.h_out);
   lya_free(ctx->get_tmp);
+  lya_free(ctx->adj.g); lya_free(ctx->adj.coef); lya_free(ctx->adj.gdw); lya_free(ctx->adj.gw);
+  lya_free(ctx->adj.out); lya_free(ctx->adj.start);
   lya_free(ctx->hist); lya_free(ctx->counts); lya_free(ctx->stats); lya_free(ctx->cta_begin);
   lya_free(ctx->cost);
   lya_free(ctx->cov);

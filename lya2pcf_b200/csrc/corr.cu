@@ -140,10 +140,8 @@ __device__ void diagonal_band(int L1, int L2, const float4* __restrict__ P1, HiL
       hi = max(hi, jhi - i);
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = min(lo, __shfl_xor_sync(FULL, lo, o));
-    hi = max(hi, __shfl_xor_sync(FULL, hi, o));
-  }
+  lo = __reduce_min_sync(FULL, lo);
+  hi = __reduce_max_sync(FULL, hi);
   m_lo = lo;
   m_hi = hi;
 }
@@ -374,12 +372,12 @@ __device__ void item_diag(const CorrParams& p, int64_t t, const SmemHist& h, typ
       const int i_hi = (m <= m_hi) ? min(L1, L2 - m) : i_lo;
       const bool nonempty = i_lo < i_hi;
       int base = nonempty ? i_lo + lane : INT_MAX;
-      for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
+      base = __reduce_min_sync(FULL, base);
       if (base == INT_MAX) continue;
       const int k_beg = i_lo + lane - base;           // lane's first step
       int stop = nonempty ? i_hi + lane - base : 0;   // lane's end (exclusive), shrinks on the rtmax stop
       int k_end = stop;
-      for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
+      k_end = __reduce_max_sync(FULL, k_end);
       const int ioff = base - lane;            // i = ioff + k   (>= -31)
       const int joff = base + mg + lane;       // j = joff + k   (>= -31)
       // lane pointers at step 0; loads run up to 34 pixels outside a forest,
@@ -614,14 +612,14 @@ __device__ void item_diag2(const CorrParams& p, int64_t t, const SmemHist& h, ty
     const int ib_lo = max(0, -mb), ib_hi = (mb <= m_hi) ? min(L1, L2 - mb) : ib_lo;
     const bool ne_a = ia_lo < ia_hi, ne_b = ib_lo < ib_hi;
     int base = min(ne_a ? ia_lo + lane : INT_MAX, ne_b ? ib_lo + lane : INT_MAX);
-    for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
+    base = __reduce_min_sync(FULL, base);
     if (base == INT_MAX) continue;
     W.ka_beg = ne_a ? ia_lo + lane - base : 0;
     W.kb_beg = ne_b ? ib_lo + lane - base : 0;
     W.stop_a = ne_a ? ia_hi + lane - base : 0;
     W.stop_b = ne_b ? ib_hi + lane - base : 0;
     int k_end = max(W.stop_a, W.stop_b);
-    for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
+    k_end = __reduce_max_sync(FULL, k_end);
     W.ioff = base - lane;             // i = ioff + k    (>= -31)
     W.joff = base + ma - lane;        // j_a = joff + k  (>= -31), j_b = j_a + 1
     const typename Tr::Ptr A1 = Tr::ptr(p, a + W.ioff);
@@ -891,7 +889,7 @@ struct LeanWalk {
         act_a = act_a && k < ka_end;
         act_b = act_b && k < kb_end;
         int ke = max(ka_end, kb_end);   // diagonals past rtmax shorten the walk
-        for (int o = 16; o > 0; o >>= 1) ke = max(ke, __shfl_xor_sync(FULL, ke, o));
+        ke = __reduce_max_sync(FULL, ke);
         kall = min(kall, ke);
       }
       if (cnt > REC - 64) {
@@ -931,14 +929,14 @@ __device__ void item_lean(const CorrParams& p, int64_t t, const SmemHist& h, Rec
     const int ib_lo = max(0, -mb), ib_hi = (mb <= m_hi) ? min(L1, L2 - mb) : ib_lo;
     const bool ne_a = ia_lo < ia_hi, ne_b = ib_lo < ib_hi;
     int base = min(ne_a ? ia_lo + lane : INT_MAX, ne_b ? ib_lo + lane : INT_MAX);
-    for (int o = 16; o > 0; o >>= 1) base = min(base, __shfl_xor_sync(FULL, base, o));
+    base = __reduce_min_sync(FULL, base);
     if (base == INT_MAX) continue;
     W.ka_beg = ne_a ? ia_lo + lane - base : 0;
     W.kb_beg = ne_b ? ib_lo + lane - base : 0;
     W.ka_end = ne_a ? ia_hi + lane - base : 0;
     W.kb_end = ne_b ? ib_hi + lane - base : 0;
     int k_end = max(W.ka_end, W.kb_end);
-    for (int o = 16; o > 0; o >>= 1) k_end = max(k_end, __shfl_xor_sync(FULL, k_end, o));
+    k_end = __reduce_max_sync(FULL, k_end);
     W.kall = k_end;
     __syncwarp();
     if (lane == 0) { ctl->base = base; ctl->mg = mg; }
@@ -969,7 +967,7 @@ __device__ void item_lean(const CorrParams& p, int64_t t, const SmemHist& h, Rec
         lean_classify(p, ctl, W.rb, lean_e(u, v), lean_s(u, v), W.kb_end, k, 1, st);
       }
       int ke = max(W.ka_end, W.kb_end);   // first runs past rtmax
-      for (int o = 16; o > 0; o >>= 1) ke = max(ke, __shfl_xor_sync(FULL, ke, o));
+      ke = __reduce_max_sync(FULL, ke);
       W.kall = min(W.kall, ke);
     }
     // steps k, k+1 per iteration: f1 pixels q1a (k), q1b (k+1); f2 pixels

@@ -45,12 +45,14 @@
 
 namespace {
 
-constexpr int DT = 512;       // threads per CTA
 constexpr int TS = 8;         // rt bins a pixel column may span
 constexpr int TSB = TS + 2;   // rows of a column being built (its window may be one bin wider at each end)
-constexpr int NW = DT / 32;   // warps per CTA
-constexpr int CH = 32;        // pixels per staged chunk of a block (a multiple of 4)
 constexpr int NP_MAX = 64;    // np of the blocks: at most 8 x 8 tiles of 8 x 8
+// Launch shapes the autotuner chooses from: threads per CTA (DT) and pixels per
+// staged chunk of a block (CH, a multiple of 4).  Shape 0 is the default.
+struct DistShape { int dt, ch; };
+constexpr DistShape DIST_SHAPES[] = {{512, 32}, {512, 16}, {512, 64}, {256, 32}, {256, 16}};
+constexpr int N_DIST_SHAPES = sizeof(DIST_SHAPES) / sizeof(DIST_SHAPES[0]);
 // Staged row length for np bins: 8 * ceil(np/8) plus 4, so the four rows of an
 // MMA fragment load fall in disjoint shared-memory banks.
 __host__ __device__ __forceinline__ int stage_npad(int np) { return 8 * ((np + 7) / 8) + 4; }
@@ -79,6 +81,8 @@ struct DistParams {
   double* W;               // [nb]
   unsigned long long* err; // [1] pixels whose column spans more than TS rt bins
   unsigned long long* next;// [1] work queue counter
+  unsigned long long* mma; // [1] FP64 tensor-core MMAs (m8n8k4) issued, for the roofline
+  int shape;               // launch shape (DIST_SHAPES index); part of the captured graph's key
 };
 
 // Bin of a pixel pair with the reference FP64 formula, as (bp, bt); false when
@@ -100,7 +104,9 @@ __device__ __forceinline__ double pair_ft(double d1, double d2, double sh, const
   return floor(__dmul_rn(__dmul_rn(__dadd_rn(d1, d2), sh), p.binner_rt));
 }
 
+template <int DT, int CH>
 __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
+  constexpr int NW = DT / 32;   // warps per CTA
   extern __shared__ __align__(16) unsigned char smem[];
   const int ML = p.max_len;
   const int np = p.np, nt = p.nt, nb = p.nb, NPAD = p.npad;
@@ -129,6 +135,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   double* BL = BS + CH * NPAD;
   const int ntile = (np + 7) / 8;   // tile rows = tile columns of a 50x50 block (7 for np = 50)
   const int grp = lane >> 2, kq = lane & 3;
+  unsigned long long n_mma = 0;     // thread 0: MMAs of this CTA
 
   for (;;) {
     if (tid == 0) s_item = (long long)atomicAdd(p.next, 1ull);
@@ -342,6 +349,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         for (int c0 = 0; c0 < n; c0 += CH) {
           const int rows = min(CH, n - c0);
           const int rows4 = (rows + 3) & ~3;   // MMA steps take 4 rows; the padding rows are zero
+          if (tid == 0) n_mma += (unsigned long long)(rows4 / 4) * ntile * ntile * 2;
           for (int r = warp; r < rows4; r += NW) {   // a warp per staged row, lanes over the bins
             const double *cs = nullptr, *cl = nullptr;
             double kS = 0.0, kL = 0.0;
@@ -431,9 +439,53 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
     }
     __syncthreads();
   }
+  if (tid == 0 && n_mma) atomicAdd(p.mma, n_mma);
 }
 
+template <int V>
+cudaError_t set_dist_smem_v(int smem) {
+  return cudaFuncSetAttribute(k_dist<DIST_SHAPES[V].dt, DIST_SHAPES[V].ch>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              smem);
+}
+
+cudaError_t set_dist_smem(int shape, int smem) {
+  switch (shape) {
+    case 1: return set_dist_smem_v<1>(smem);
+    case 2: return set_dist_smem_v<2>(smem);
+    case 3: return set_dist_smem_v<3>(smem);
+    case 4: return set_dist_smem_v<4>(smem);
+    default: return set_dist_smem_v<0>(smem);
+  }
+}
+
+template <int V>
+cudaError_t launch_dist_v(int grid, size_t smem, cudaStream_t s, const DistParams& p) {
+  k_dist<DIST_SHAPES[V].dt, DIST_SHAPES[V].ch><<<grid, DIST_SHAPES[V].dt, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dist(int shape, int grid, size_t smem, cudaStream_t s, const DistParams& p) {
+  switch (shape) {
+    case 1: return launch_dist_v<1>(grid, smem, s, p);
+    case 2: return launch_dist_v<2>(grid, smem, s, p);
+    case 3: return launch_dist_v<3>(grid, smem, s, p);
+    case 4: return launch_dist_v<4>(grid, smem, s, p);
+    default: return launch_dist_v<0>(grid, smem, s, p);
+  }
+}
+static_assert(N_DIST_SHAPES == 5, "the launch tables above cover every shape");
+
 }  // namespace
+
+extern "C" int lya_dist_config(lya_ctx* ctx, int32_t shape, int64_t max_items) {
+  if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_dist_config: ctx is NULL");
+  if (shape < 0 || shape >= N_DIST_SHAPES)
+    return lya_fail(ctx, LYA_ERR_ARG, "lya_dist_config: shape %d outside [0,%d)", shape, N_DIST_SHAPES);
+  if (max_items < 0) return lya_fail(ctx, LYA_ERR_ARG, "lya_dist_config: max_items < 0");
+  ctx->dist_shape = shape;
+  ctx->dist_max_items = max_items;
+  return LYA_OK;
+}
 
 extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   if (!ctx) return lya_fail(nullptr, LYA_ERR_ARG, "lya_dist_run: ctx is NULL");
@@ -449,11 +501,14 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     max_len = std::max<int>(max_len, (int)(ctx->h_start[f + 1] - ctx->h_start[f]));
   if (max_len > 65535) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests longer than 65535 pixels");
   const int npad = stage_npad(np);
+  const int shape = ctx->dist_shape;
+  const int DT = DIST_SHAPES[shape].dt, CH = DIST_SHAPES[shape].ch, NW = DT / 32;
   const size_t stage_len = std::max<size_t>((size_t)4 * CH * npad, (size_t)NW * 2 * TSB * np);
   const size_t smem = sizeof(double) * (10 * (size_t)max_len + stage_len) +
                       sizeof(int) * (6 * (size_t)max_len);
   if (smem > 227 * 1024)
-    return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory", max_len, smem);
+    return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory (shape %d)",
+                    max_len, smem, shape);
   const int grid = ctx->num_sms;
   // scratch and outputs kept in the context, so later calls (one per healpix
   // pixel in the drop-in driver) allocate nothing and replay the captured graph
@@ -466,7 +521,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     if (e == cudaSuccess) e = lya_alloc(&ds.W, nb);
     if (e == cudaSuccess) e = lya_alloc(&ds.col, (size_t)grid * 2 * 2 * max_len * TS * np);
     if (e == cudaSuccess) e = lya_alloc(&ds.mom, (size_t)grid * 4 * nt * np);
-    if (e == cudaSuccess) e = lya_alloc(&ds.err, 3);
+    if (e == cudaSuccess) e = lya_alloc(&ds.err, 4);
     if (e != cudaSuccess) {
       lya_free(ds.D); lya_free(ds.W); lya_free(ds.col); lya_free(ds.mom); lya_free(ds.err);
       ds = DistScratch{};
@@ -475,7 +530,8 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     ds.nb = nb; ds.max_len = max_len; ds.grid = grid;
   }
   cudaStream_t s = ctx->stream;
-  const long long n_items = ctx->wq.n_pairs;
+  const long long n_items = ctx->dist_max_items > 0 ? std::min<long long>(ctx->wq.n_pairs, ctx->dist_max_items)
+                                                    : ctx->wq.n_pairs;
   DistParams p;
   memset(&p, 0, sizeof(p));   // padding bytes take part in the graph key
   p.pix8 = ctx->cat.pix8; p.dl = ctx->cat.dl; p.pstart = ctx->cat.pstart; p.len = ctx->cat.len;
@@ -485,21 +541,23 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   p.binner_rp = (double)np / ctx->rpmax; p.binner_rt = (double)nt / ctx->rtmax;
   p.np = np; p.nt = nt; p.nb = nb; p.cos_variant = ctx->cos_variant; p.npad = npad;
   p.col = ds.col; p.moments = ds.mom; p.D = ds.D; p.W = ds.W; p.err = ds.err; p.next = ds.err + 1;
+  p.mma = ds.err + 3;
+  p.shape = shape;
   const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len) + sizeof(int) * (6 * (size_t)ds.max_len);
   static_assert(sizeof(DistParams) <= sizeof(ds.key), "graph key does not fit");
   cudaError_t e = cudaSuccess;
   if (!ds.graph || memcmp(ds.key, &p, sizeof(p)) != 0) {
     if (ds.graph) { cudaGraphExecDestroy(ds.graph); ds.graph = nullptr; }
-    e = cudaFuncSetAttribute(k_dist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_run);
+    e = set_dist_smem(shape, (int)smem_run);
     cudaGraph_t g = nullptr;
     if (e == cudaSuccess) e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       cudaError_t eq = cudaMemsetAsync(ds.D, 0, sizeof(double) * (size_t)nb * nb, s);
       if (eq == cudaSuccess) eq = cudaMemsetAsync(ds.W, 0, sizeof(double) * nb, s);
       if (eq == cudaSuccess) eq = cudaMemsetAsync(ds.err, 0, 2 * sizeof(unsigned long long), s);
+      if (eq == cudaSuccess) eq = cudaMemsetAsync(ds.err + 3, 0, sizeof(unsigned long long), s);
       if (eq == cudaSuccess) {
-        k_dist<<<grid, DT, smem_run, s>>>(p);
-        eq = cudaGetLastError();
+        eq = launch_dist(shape, grid, smem_run, s, p);
       }
       const cudaError_t ec = cudaStreamEndCapture(s, &g);
       e = eq != cudaSuccess ? eq : ec;
@@ -519,8 +577,9 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     ctx->launches++;
     e = cudaEventRecord(ctx->ev1, s);
   }
-  unsigned long long nerr = 0;
+  unsigned long long nerr = 0, nmma = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nerr, ds.err, sizeof(nerr), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nmma, ds.err + 3, sizeof(nmma), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && D) e = cudaMemcpyAsync(D, ds.D, sizeof(double) * (size_t)nb * nb, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && W) e = cudaMemcpyAsync(W, ds.W, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -528,6 +587,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   if (e == cudaSuccess) cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   if (e != cudaSuccess) return lya_fail(ctx, LYA_ERR_CUDA, "lya_dist_run: %s", cudaGetErrorString(e));
   ctx->last.kernel_ms = ms;
+  ctx->last.dist_mma_flops = (double)nmma * 2.0 * 8 * 8 * 4;   // m8n8k4: 256 FMA per MMA
   if (nerr) return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: %llu pixels pair into more than %d rt bins", nerr, TS);
   return LYA_OK;
 }

@@ -137,6 +137,18 @@ struct SelectScratch {
   double* h_out = nullptr;      // pinned [3]: kept count (as long long bits), tot
 };
 
+// Scratch of lya_corr_adjoint (kept between calls, grown, never shrunk).
+struct AdjScratch {
+  double* g = nullptr;          // [nb] g on the device
+  double* coef = nullptr;       // [2][nb] g/W, -g xi/W
+  double* gdw = nullptr;        // [npad] gradients, padded layout
+  double* gw = nullptr;
+  double* out = nullptr;        // [npix] unpadded copy for host outputs
+  int64_t* start = nullptr;     // [n + 1] CSR offsets
+  int nb = 0;
+  int64_t n = 0, npad = 0, npix = 0;
+};
+
 struct lya_ctx {
   int device = 0;
   int num_sms = 148;
@@ -161,6 +173,7 @@ struct lya_ctx {
   WorkQueue wq;
   NbrScratch nbr;
   SelectScratch sel;
+  AdjScratch adj;
   int cos_variant = 0;
 
   // correlation outputs: per slot, LYA_NQ quantities as (hi, lo) FP64 pairs,
@@ -191,6 +204,8 @@ struct lya_ctx {
   bool inject_device_error = false;      // test hook: the next run's pair kernel raises its error flag
 
   DistScratch dist;
+  int32_t dist_shape = 0;                // lya_dist_config: launch shape of the distortion kernel
+  int64_t dist_max_items = 0;            // lya_dist_config: 0 = every forest pair, else the first n
 
   // covariance post-processing: the last covariance, kept for lya_covariance_smooth
   double* cov = nullptr;                 // [cov_nb][cov_nb]

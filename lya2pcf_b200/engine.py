@@ -236,20 +236,42 @@ class PairEngine:
 
     def adjoint(self, g, out_dw=None, out_w=None):
         """Gradient of sum_b g_b DW_b/W_b w.r.t. dw and w of every pixel (CSR
-        order), bins held fixed.  ``out_dw``/``out_w`` may be CUDA torch tensors
-        (float64, contiguous, on this context's device) to receive the result on
-        the device; otherwise numpy arrays are returned."""
-        g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1)
-        if g.size != self.nb:
-            raise ValueError(f'g must have {self.nb} entries')
+        order), bins held fixed.  ``g`` is a numpy array or a CUDA float64
+        torch tensor on this context's device.  ``out_dw``/``out_w`` may be
+        CUDA torch tensors (float64, contiguous, on this context's device) to
+        receive the result on the device; otherwise numpy arrays are returned."""
+        flags = 0
+        if hasattr(g, 'data_ptr'):
+            if g.numel() != self.nb:
+                raise ValueError(f'g must have {self.nb} entries')
+            gp = C.c_void_p(g.data_ptr())
+            flags |= 2
+        else:
+            g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1)
+            if g.size != self.nb:
+                raise ValueError(f'g must have {self.nb} entries')
+            gp = N.ptr(g)
         if out_dw is not None:
-            self._check(self.lib.lya_corr_adjoint(self.ctx, N.ptr(g), C.c_void_p(out_dw.data_ptr()),
-                                                  C.c_void_p(out_w.data_ptr()), 1))
+            self._check(self.lib.lya_corr_adjoint(self.ctx, gp, C.c_void_p(out_dw.data_ptr()),
+                                                  C.c_void_p(out_w.data_ptr()), flags | 1))
             return out_dw, out_w
         gdw = np.zeros(self.fs.npix_total, dtype=np.float64)
         gw = np.zeros(self.fs.npix_total, dtype=np.float64)
-        self._check(self.lib.lya_corr_adjoint(self.ctx, N.ptr(g), N.ptr(gdw), N.ptr(gw), 0))
+        self._check(self.lib.lya_corr_adjoint(self.ctx, gp, N.ptr(gdw), N.ptr(gw), flags))
         return gdw, gw
+
+    def totals(self, out_w=None, out_dw=None):
+        """``(W[nb], DW[nb])``: sum w1w2 and sum dw1dw2 over every owner slot of
+        the last :meth:`run`.  With CUDA float64 torch tensors ``out_w`` and
+        ``out_dw`` (on this context's device) the totals stay on the device."""
+        if out_w is not None:
+            self._check(self.lib.lya_corr_totals(self.ctx, C.c_void_p(out_w.data_ptr()),
+                                                 C.c_void_p(out_dw.data_ptr()), 1))
+            return out_w, out_dw
+        W = np.zeros(self.nb)
+        DW = np.zeros(self.nb)
+        self._check(self.lib.lya_corr_totals(self.ctx, N.ptr(W), N.ptr(DW), 0))
+        return W, DW
 
     def update_weights(self, w, dw):
         """Replace w and dw of every pixel (numpy arrays, or CUDA float64 torch
@@ -268,6 +290,32 @@ class PairEngine:
         W = np.zeros(self.nb, dtype=np.float64)
         self._check(self.lib.lya_dist_run(self.ctx, N.ptr(D), N.ptr(W)))
         return D, W
+
+    DIST_SHAPES = ((512, 32), (512, 16), (512, 64), (256, 32), (256, 16))   # lya_dist_config shapes
+
+    def autotune_distortion(self, fraction=0.05, min_items=2000):
+        """Choose the distortion kernel's launch shape (threads per CTA, pixels
+        per staged chunk) for this catalogue: time every shape on the first
+        ``fraction`` of the work queue (at least ``min_items`` forest pairs;
+        the second of two runs, i.e. the replayed graph) and keep the fastest
+        for later :meth:`distortion` calls.  Shapes whose shared memory does not
+        fit the catalogue's longest forest are skipped.  Returns the timings."""
+        n = max(min_items, int(self.n_pairs * fraction))
+        timings = []
+        for shape in range(len(self.DIST_SHAPES)):
+            self._check(self.lib.lya_dist_config(self.ctx, shape, n))
+            try:
+                for _ in range(2):
+                    self._check(self.lib.lya_dist_run(self.ctx, None, None))
+            except N.LyaError as err:
+                timings.append({'shape': shape, 'error': str(err)})
+                continue
+            timings.append({'shape': shape, 'threads': self.DIST_SHAPES[shape][0],
+                            'chunk': self.DIST_SHAPES[shape][1], 'kernel_ms': self.stats()['kernel_ms']})
+        ok = [t for t in timings if 'kernel_ms' in t]
+        best = min(ok, key=lambda t: t['kernel_ms'])['shape'] if ok else 0
+        self._check(self.lib.lya_dist_config(self.ctx, best, 0))
+        return {'best': best, 'items': n, 'timings': timings}
 
     def covariance(self, smooth=True):
         """Covariance of the per-owner-slot correlation estimates xi = DW/W of

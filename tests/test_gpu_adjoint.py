@@ -2,7 +2,10 @@
 
 Checked against the oracle's FP64 adjoint and against central finite
 differences (eps = 1e-6, float64) on the 500-forest, 10 deg^2 configuration
-(scaled): tolerance 1e-5 of the gradient's largest component."""
+(forests of 100-300 pixels): tolerance 1e-5 of the gradient's largest
+component.  The float32 path (float32 w and delta in, float32 gradients out)
+is checked against the float64 path at the same float32-representable inputs:
+1e-5 of the gradient's largest component."""
 import numpy as np
 import pytest
 import torch
@@ -18,7 +21,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope='module')
 def cfg4():
-    fs = synthetic.make(4, n=200)
+    fs = synthetic.make(4)
+    assert fs.n == 500 and fs.lengths.min() >= 100 and fs.lengths.max() <= 300
     am = synthetic.angmax_for(fs)
     eng = PairEngine().upload(fs)
     eng.build_pairs(am)
@@ -83,3 +87,44 @@ def test_autograd_matches_finite_differences(cfg4):
             # forward's rounding noise, ~1e-10 after dividing by 2 eps, sets
             # the floor for the smallest components)
             assert abs(fd - an) <= 1e-5 * max(abs(fd), scale[which]), (which, int(p), fd, an)
+
+
+def test_totals_equal_summed_histograms(cfg4):
+    fs, am, eng = cfg4
+    eng.update_weights(fs.w, fs.dw)
+    eng.run(kernel=N.KERNEL_FP32_GUARDED)
+    hist, _ = eng.histograms()
+    W, DW = eng.totals()
+    np.testing.assert_allclose(W, hist[:, N.Q_W].sum(0), rtol=1e-13, atol=0)
+    np.testing.assert_allclose(DW, hist[:, N.Q_DW].sum(0), rtol=1e-12, atol=1e-13 * np.abs(DW).max())
+    tW = torch.empty(eng.nb, dtype=torch.float64, device='cuda')
+    tDW = torch.empty_like(tW)
+    eng.totals(out_w=tW, out_dw=tDW)
+    assert np.array_equal(tW.cpu().numpy(), W) and np.array_equal(tDW.cpu().numpy(), DW)
+
+
+def test_float32_path_matches_float64_path(cfg4):
+    """float32 w and delta: xi and the gradients (float32) equal the float64
+    path's at the same (float32-representable) inputs to 1e-5 of their
+    largest component."""
+    fs, am, eng = cfg4
+    dev = torch.device('cuda')
+    fid = forest_index(fs.start, dev)
+    rng = np.random.default_rng(8)
+    loglam = torch.as_tensor(np.log10((1 + fs.z) * 1215.67), device=dev)
+    delta32 = torch.as_tensor(rng.normal(0, 0.25, fs.npix_total).astype(np.float32), device=dev)
+    w32 = torch.as_tensor(fs.w.astype(np.float32), device=dev)
+    g = torch.as_tensor(rng.normal(size=eng.nb), device=dev)
+    out = {}
+    for dt in (torch.float32, torch.float64):
+        w = w32.to(dt).clone().requires_grad_(True)
+        delta = delta32.to(dt).clone().requires_grad_(True)
+        dw = project_delta(w, delta, loglam.to(dt), fid, fs.n)
+        x = xi(w, dw, eng)
+        L = torch.sum(g.to(dt) * x)
+        gw, gd = torch.autograd.grad(L, (w, delta))
+        assert x.dtype == dt and gw.dtype == dt and gd.dtype == dt
+        out[dt] = (x.detach().double(), gw.double(), gd.double())
+    for k in range(3):
+        a, b = out[torch.float32][k], out[torch.float64][k]
+        assert float((a - b).abs().max()) <= 1e-5 * float(b.abs().max()), k

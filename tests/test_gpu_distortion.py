@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import edge_cases as E
+from lya2pcf_b200 import _native as N
 from lya2pcf_b200 import synthetic
 from lya2pcf_b200.dropin_path import ensure_on_path
 from lya2pcf_b200.engine import PairEngine
@@ -146,3 +147,29 @@ def test_multiple_data_driver_per_file_and_merged(tmp_path):
             Wh += W
     assert 0 < Wh.sum() < Wp.sum()
     _check_ratio(out['half'], Dh, Wh)
+
+
+def test_every_launch_shape_and_the_item_limit():
+    """Every launch shape of the distortion kernel (lya_dist_config) gives the
+    oracle's D and W; a limit of n items bins exactly the first n forest pairs;
+    the autotuner leaves a working shape selected."""
+    fs = synthetic.make(3, n=70)
+    am = synthetic.angmax_for(fs)
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.build_pairs(am)
+        f1, f2 = eng.get_pairs()
+        Do, Wo = O.distortion(fs, f1, f2)
+        for shape in range(len(PairEngine.DIST_SHAPES)):
+            N.check(eng.lib.lya_dist_config(eng.ctx, shape, 0), eng.ctx)
+            D, W = eng.distortion()
+            _check(D, W, Do, Wo)
+        n = len(f1) // 3
+        N.check(eng.lib.lya_dist_config(eng.ctx, 0, n), eng.ctx)
+        D, W = eng.distortion()
+        Dn, Wn = O.distortion(fs, f1[:n], f2[:n])
+        _check(D, W, Dn, Wn)
+        tune = eng.autotune_distortion(fraction=0.5, min_items=10)
+        assert 0 <= tune['best'] < len(PairEngine.DIST_SHAPES)
+        D, W = eng.distortion()
+        _check(D, W, Do, Wo)
