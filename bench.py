@@ -412,7 +412,7 @@ def run_b200(args, dist):
                        'algorithmic_bytes_per_launch': algo_bytes,
                        'note': 'not the bound: per forest pair the kernel reads (len1+len2) x 24 B algorithmically, '
                                're-read from L2'}
-        roof['smem_atomic'] = smem_atomic_term(st, kms)
+        roof['smem_atomic'] = smem_atomic_term(st, kms, dev)
         cpu = None if args.no_cpu_baseline else cpu_baseline(fs, angmax, args.cpu_seconds)
         distortion = None if args.dist_scale <= 0 else distortion_sample(args.dist_scale, dev)
         ms_step = t_max / args.steps
@@ -650,63 +650,29 @@ def alu_roofline(st, kms, clk):
             'peak_source': 'computed: 148 SMs x 128 FP32 lanes x sampled SM clock / 17 ops per pair (not measured)'}
 
 
-def smem_atomic_term(st, kms):
+def smem_atomic_term(st, kms, dev):
     """The shared-memory atomic term of the bound: the reference algorithm does
     6 shared atomics (5 FP64 sums and a count) per in-range pixel pair; the
-    kernel does 6 per run of pairs that share a bin.  Peak atomic rate from the
-    committed probe measurement (profiles/smem_atomic_rate.json)."""
-    try:
-        prof = json.load(open(os.path.join(ROOT, 'profiles', 'smem_atomic_rate.json')))
-        rate = float(prof['f64_add_random_bins_per_s'])
-    except Exception:
-        return None
+    kernel does 6 per run of pairs that share a bin.  Peak atomic rate measured
+    here by the library's probe (lya_probe_smem_atomics, FP64 adds into random
+    bins of a 2500-bin histogram)."""
+    from lya2pcf_b200 import _native as N
+    rates = np.zeros(3)
+    N.check(N.load().lya_probe_smem_atomics(int(dev), N.ptr(rates)))
+    rate = float(rates[1])
     evals = max(st['evaluated_pairs'], 1.0)
     f_in = st['in_range_pairs'] / evals
     per_pair_ref = 6.0 * f_in
     per_pair_kernel = 6.0 * st['runs_flushed'] / evals
-    return {'peak_atomics_per_s': rate, 'source': 'measured probe, FP64 shared atomicAdd into random bins of a '
-                                                  '2500-bin histogram (profiles/smem_atomic_rate.md)',
+    return {'peak_atomics_per_s': rate, 'probe_rates_per_s': {'f64_distinct': float(rates[0]),
+                                                              'f64_random_bins': rate,
+                                                              'u32_distinct': float(rates[2])},
+            'source': 'measured in this run: lya_probe_smem_atomics, FP64 shared atomicAdd into random bins',
             'in_range_fraction': f_in,
             'bound_pair_evals_per_s_reference_form': rate / per_pair_ref if per_pair_ref else None,
             'atomics_per_evaluated_pair': per_pair_kernel,
             'bound_pair_evals_per_s_this_kernel': rate / per_pair_kernel if per_pair_kernel else None,
             'atomic_time_fraction': (st['runs_flushed'] * 6.0 / rate) / (kms * 1e-3)}
-
-
-def profile_case(args):
-    """One pass of the pair kernel, the distortion kernel or the adjoint on a
-    catalogue of configuration ``args.config`` at ``args.scale``, after one
-    warm-up pass; prints the library's statistics as one JSON line."""
-    from lya2pcf_b200 import synthetic
-    from lya2pcf_b200.engine import PairEngine
-    fs = synthetic.make(args.config, scale=args.scale)
-    kern = KERNEL_CODES[args.kernel]
-    with PairEngine() as eng:
-        eng.upload(fs)
-        eng.build_pairs(synthetic.angmax_for(fs))
-        if args.profile_case == 'dist':
-            tune = eng.autotune_distortion()
-            eng.distortion()
-            t = time.perf_counter()
-            eng.distortion()
-            st = eng.stats()
-            st['dist_wall_s'] = time.perf_counter() - t
-            st['tuned'] = tune
-            st['forest_pairs'] = eng.n_pairs
-        elif args.profile_case == 'adjoint':
-            eng.run(kernel=kern, guard=GUARD)
-            g = np.random.default_rng(4).normal(size=eng.nb)
-            eng.adjoint(g)
-            t = time.perf_counter()
-            eng.adjoint(g)
-            st = eng.stats()
-            st['adjoint_wall_s'] = time.perf_counter() - t
-        else:
-            eng.run(kernel=kern, guard=GUARD, variant=args.variant)
-            st = eng.run(kernel=kern, guard=GUARD, variant=args.variant)
-        st['npix_total'] = fs.npix_total
-        st['case'] = {'kernel': args.profile_case, 'config': args.config, 'scale': args.scale, 'forests': fs.n}
-        print(json.dumps(st), flush=True)
 
 
 def main():

@@ -258,6 +258,14 @@ int lya_corr_pixel_noalloc(int device, const double* dc, const double* w, const 
 int lya_debug_fail_alloc(int64_t after);
 int lya_debug_inject(lya_ctx* ctx, int32_t what);
 
+/* Shared-memory atomic throughput of `device` (no counterpart in the
+ * reference): rates[0] FP64 atomicAdd at distinct addresses within a warp,
+ * rates[1] FP64 atomicAdd into pseudo-random bins of a 2500-bin histogram,
+ * rates[2] 32-bit integer atomicAdd at distinct addresses, in atomics per
+ * second over the whole GPU (one-wave grid of 512-thread CTAs).  The
+ * shared-atomic term of the pair kernel's roofline. */
+int lya_probe_smem_atomics(int device, double* rates);
+
 /* Device timer on the context's stream: op 0 records the start event, op 1
  * records the stop event, waits for it and writes the elapsed milliseconds. */
 int lya_timer(lya_ctx* ctx, int32_t op, double* ms);

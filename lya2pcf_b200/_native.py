@@ -39,6 +39,7 @@ SIGNATURES = {
     'lya_select_slots': ([P, P], C.c_int),
     'lya_debug_fail_alloc': ([C.c_int64], C.c_int),
     'lya_debug_inject': ([P, C.c_int32], C.c_int),
+    'lya_probe_smem_atomics': ([C.c_int, P], C.c_int),
     'lya_corr_run': ([P, P], C.c_int),
     'lya_corr_get': ([P, C.c_int32, C.c_int32, P, P], C.c_int),
     'lya_corr_adjoint': ([P, P, P, P, C.c_int32], C.c_int),

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'liblya2pcf.so')
-SOURCES = ['context.cu', 'pairs.cu', 'corr.cu', 'adjoint.cu', 'distortion.cu', 'covariance.cu', 'noalloc.cu']
+SOURCES = ['context.cu', 'pairs.cu', 'corr.cu', 'adjoint.cu', 'distortion.cu', 'covariance.cu', 'noalloc.cu', 'probe.cu']
 
 NVCC_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-lineinfo', '-std=c++17',
               '-Xcompiler', '-fPIC', '-cudart', 'static', '--expt-relaxed-constexpr']

@@ -5,7 +5,9 @@ differences (eps = 1e-6, float64) on the 500-forest, 10 deg^2 configuration
 (forests of 100-300 pixels): tolerance 1e-5 of the gradient's largest
 component.  The float32 path (float32 w and delta in, float32 gradients out)
 is checked against the float64 path at the same float32-representable inputs:
-1e-5 of the gradient's largest component."""
+1e-4 of the largest component (the float32 projection of delta rounds dw at
+2^-24, and xi sums dw products of random sign, so its float32 error relative
+to max |xi| is ~1e-5)."""
 import numpy as np
 import pytest
 import torch
@@ -105,7 +107,7 @@ def test_totals_equal_summed_histograms(cfg4):
 
 def test_float32_path_matches_float64_path(cfg4):
     """float32 w and delta: xi and the gradients (float32) equal the float64
-    path's at the same (float32-representable) inputs to 1e-5 of their
+    path's at the same (float32-representable) inputs to 1e-4 of their
     largest component."""
     fs, am, eng = cfg4
     dev = torch.device('cuda')
@@ -127,4 +129,4 @@ def test_float32_path_matches_float64_path(cfg4):
         out[dt] = (x.detach().double(), gw.double(), gd.double())
     for k in range(3):
         a, b = out[torch.float32][k], out[torch.float64][k]
-        assert float((a - b).abs().max()) <= 1e-5 * float(b.abs().max()), k
+        assert float((a - b).abs().max()) <= 1e-4 * float(b.abs().max()), k

@@ -72,7 +72,7 @@ def test_config0_all_slots_match_oracle(cfg0, cfg0_oracle, kern, var):
     the oracle, sums within the kernel's tolerance."""
     fs, am, eng, _, (f1, f2, sis, pixels) = cfg0
     ho, co = cfg0_oracle
-    assert len(pixels) >= 30
+    assert len(pixels) >= 15   # the 100 deg^2 patch covers 17 healpix pixels at nside 16
     eng.run(kernel=kern, variant=var)
     h, c = eng.histograms()
     check_hist(h, c, ho, co, kern, f'kernel {kern}')
