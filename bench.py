@@ -675,6 +675,42 @@ def smem_atomic_term(st, kms, dev):
             'atomic_time_fraction': (st['runs_flushed'] * 6.0 / rate) / (kms * 1e-3)}
 
 
+def profile_case(args):
+    """One pass of the pair kernel, the distortion kernel or the adjoint on a
+    catalogue of configuration ``args.config`` at ``args.scale``, after one
+    warm-up pass; prints the library's statistics as one JSON line."""
+    from lya2pcf_b200 import synthetic
+    from lya2pcf_b200.engine import PairEngine
+    fs = synthetic.make(args.config, scale=args.scale)
+    kern = KERNEL_CODES[args.kernel]
+    with PairEngine() as eng:
+        eng.upload(fs)
+        eng.build_pairs(synthetic.angmax_for(fs))
+        if args.profile_case == 'dist':
+            tune = eng.autotune_distortion()
+            eng.distortion()
+            t = time.perf_counter()
+            eng.distortion()
+            st = eng.stats()
+            st['dist_wall_s'] = time.perf_counter() - t
+            st['tuned'] = tune
+            st['forest_pairs'] = eng.n_pairs
+        elif args.profile_case == 'adjoint':
+            eng.run(kernel=kern, guard=GUARD)
+            g = np.random.default_rng(4).normal(size=eng.nb)
+            eng.adjoint(g)
+            t = time.perf_counter()
+            eng.adjoint(g)
+            st = eng.stats()
+            st['adjoint_wall_s'] = time.perf_counter() - t
+        else:
+            eng.run(kernel=kern, guard=GUARD, variant=args.variant)
+            st = eng.run(kernel=kern, guard=GUARD, variant=args.variant)
+        st['npix_total'] = fs.npix_total
+        st['case'] = {'kernel': args.profile_case, 'config': args.config, 'scale': args.scale, 'forests': fs.n}
+        print(json.dumps(st), flush=True)
+
+
 def main():
     args = parse()
     if args.split:   # the extras below describe one catalogue on one GPU; a split run measures the step only

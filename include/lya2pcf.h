@@ -190,7 +190,7 @@ int lya_update_weights(lya_ctx* ctx, const double* w, const double* dw, int32_t 
 int lya_dist_run(lya_ctx* ctx, double* D, double* W);
 
 /* Launch shape of lya_dist_run's kernel (0 = default: 512 threads per CTA,
- * rows staged 32 pixels at a time; 1..4 = 512/16, 512/64, 256/32, 256/16) and
+ * rows staged 32 pixels at a time; 1..4 = 512/16, 512/24, 256/32, 256/16) and
  * an optional limit: max_items > 0 bins only the first max_items forest pairs
  * of the work queue (a timing sample for the autotuner), 0 = all.  Stays in
  * effect for later calls.  No reference counterpart. */

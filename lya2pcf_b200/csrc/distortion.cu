@@ -37,6 +37,8 @@
 // symmetric).
 // A forest whose sum w dl^2 is 0 has no slope to project out: its slope terms
 // are 0.
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -51,11 +53,20 @@ constexpr int NP_MAX = 64;    // np of the blocks: at most 8 x 8 tiles of 8 x 8
 // Launch shapes the autotuner chooses from: threads per CTA (DT) and pixels per
 // staged chunk of a block (CH, a multiple of 4).  Shape 0 is the default.
 struct DistShape { int dt, ch; };
-constexpr DistShape DIST_SHAPES[] = {{512, 32}, {512, 16}, {512, 64}, {256, 32}, {256, 16}};
+constexpr DistShape DIST_SHAPES[] = {{512, 32}, {512, 16}, {512, 24}, {256, 32}, {256, 16}};
 constexpr int N_DIST_SHAPES = sizeof(DIST_SHAPES) / sizeof(DIST_SHAPES[0]);
 // Staged row length for np bins: 8 * ceil(np/8) plus 4, so the four rows of an
 // MMA fragment load fall in disjoint shared-memory banks.
 __host__ __device__ __forceinline__ int stage_npad(int np) { return 8 * ((np + 7) / 8) + 4; }
+// Row stride of the column scratch: np rounded up to even, so every row starts
+// on a 16-byte boundary (the asynchronous 16-byte copies of the staging).
+__host__ __device__ __forceinline__ int col_stride(int np) { return (np + 1) & ~1; }
+// Shared-memory doubles of the staging area: two buffers of four [CH][NPAD]
+// row sets (double buffering), or the per-warp column builders of phase 1.
+__host__ __device__ __forceinline__ int stage_doubles(int CH, int NW, int np) {
+  const int a = 2 * 4 * CH * stage_npad(np), b = NW * 2 * (TS + 2) * np;
+  return a > b ? a : b;
+}
 
 struct DistParams {
   const double4* __restrict__ pix8;   // (dc, w, dw, z)
@@ -75,7 +86,7 @@ struct DistParams {
   double binner_rp, binner_rt;
   int np, nt, nb, cos_variant;
   int npad;                // staged row length (stage_npad(np))
-  double* col;             // scratch [grid][2 sides][max_len][TS][np] x {S, L}
+  double* col;             // scratch [grid][2 sides][max_len][TS][col_stride(np)] x {S, L}
   double* moments;         // scratch [grid][4][nt][np]: moments of the window's bins
   double* D;               // [nb][nb]
   double* W;               // [nb]
@@ -107,6 +118,9 @@ __device__ __forceinline__ double pair_ft(double d1, double d2, double sh, const
 template <int DT, int CH>
 __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   constexpr int NW = DT / 32;   // warps per CTA
+  // accumulator fragments per MMA warp: with 16 warps or more, two warps share a
+  // tile row (np <= 64: at most 8 tile columns, 4 each); otherwise one warp per row
+  constexpr int CC = NW >= 16 ? 4 : 8;
   extern __shared__ __align__(16) unsigned char smem[];
   const int ML = p.max_len;
   const int np = p.np, nt = p.nt, nb = p.nb, NPAD = p.npad;
@@ -116,24 +130,28 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   double* ksc = sl + 2 * ML;                             // [2][ML] column-product weights k_S of a pixel
   double* klc = ksc + 2 * ML;                            // [2][ML] and k_L
   double* mom = p.moments + (size_t)blockIdx.x * 4 * nt * np;   // [4][nt][np] (CTA-private, L2-resident)
-  double* stage = klc + 2 * ML;                          // [4][CH][NPAD] staged rows, or the column builders
-  const int stage_len = max(4 * CH * NPAD, NW * 2 * TSB * np);
-  int* tlo = reinterpret_cast<int*>(stage + stage_len);  // [2][ML]
+  double* stage = klc + 2 * ML;                          // 2 x [4][CH][NPAD] staged rows, or the column builders
+  const int stage_len = stage_doubles(CH, NW, np);
+  double* kbuf = stage + stage_len;                      // [2][2][CH] per staged row: k_S, k_L
+  int* tlo = reinterpret_cast<int*>(kbuf + 4 * CH);      // [2][ML]
   int* span = tlo + 2 * ML;                              // [2][ML]
   int* plist = span + 2 * ML;                            // [2*ML] packed (side << 16 | pixel)
   __shared__ int s_T0, s_T1, s_maxspan, s_cnt;
   __shared__ long long s_item;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* colS = p.col + (size_t)blockIdx.x * 2 * 2 * ML * TS * np;   // [2 sides][ML][TS][np]
-  double* colL = colS + (size_t)2 * ML * TS * np;
+  const int NS = col_stride(np);
+  double* colS = p.col + (size_t)blockIdx.x * 2 * 2 * ML * TS * NS;   // [2 sides][ML][TS][NS]
+  double* colL = colS + (size_t)2 * ML * TS * NS;
   double* myS = stage + (size_t)warp * 2 * TSB * np;
   double* myL = myS + TSB * np;
-  double* AS = stage;                  // [CH][NPAD] rows of bin t, scaled by k_S
-  double* AL = AS + CH * NPAD;         // [CH][NPAD] rows of bin t, scaled by k_L
-  double* BS = AL + CH * NPAD;         // [CH][NPAD] rows of bin u
-  double* BL = BS + CH * NPAD;
   const int ntile = (np + 7) / 8;   // tile rows = tile columns of a 50x50 block (7 for np = 50)
+  // MMA warps: tile row (w mod ntile) and, with two warps per tile row, one
+  // half of the tile columns each
+  const int nsplit = CC == 4 ? 2 : 1;
+  const int trow = warp % ntile, thalf = warp / ntile;
+  const int ccols = (ntile + nsplit - 1) / nsplit, cbeg = thalf * ccols, cend = min(ntile, cbeg + ccols);
+  const bool mma_warp = warp < ntile * nsplit;
   const int grp = lane >> 2, kq = lane & 3;
   unsigned long long n_mma = 0;     // thread 0: MMAs of this CTA
 
@@ -178,8 +196,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
       const double* dO = sd + (1 - side) * ML;
       const double* wO = sw + (1 - side) * ML;
       const double* lO = sl + (1 - side) * ML;
-      double* cS = colS + (size_t)side * ML * TS * np;
-      double* cL = colL + (size_t)side * ML * TS * np;
+      double* cS = colS + (size_t)side * ML * TS * NS;
+      double* cL = colL + (size_t)side * ML * TS * NS;
       for (int m = warp; m < Lm; m += NW) {
         const double d = dm[m];
         int jlo = 0, jhi = Lo;
@@ -292,10 +310,14 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         __syncwarp();
         if (sp > 0) {
           // rows lo..hi of the built window go to the CTA's scratch
-          double* rs = cS + (size_t)m * TS * np;
-          double* rl = cL + (size_t)m * TS * np;
+          double* rs = cS + (size_t)m * TS * NS;
+          double* rl = cL + (size_t)m * TS * NS;
           const int off = (lo - wlo) * np;
-          for (int q = lane; q < sp * np; q += 32) { rs[q] = myS[off + q]; rl[q] = myL[off + q]; }
+          for (int q = lane; q < sp * NS; q += 32) {
+            const int row = q / NS, col = q - row * NS;
+            rs[q] = col < np ? myS[off + row * np + col] : 0.0;
+            rl[q] = col < np ? myL[off + row * np + col] : 0.0;
+          }
           if (lane == 0) {
             atomicMin(&s_T0, lo);
             atomicMax(&s_T1, lo + sp - 1);
@@ -317,9 +339,14 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
     }
     __syncthreads();
     const double cA = 1.0 / (om1 * om2), cB = io2 / om1, cC = io1 / om2, cD = io1 * io2;
-    // ---- phase 2: blocks (t, u), T0 <= t <= u <= T1, diagonal blocks first
+    // ---- phase 2: blocks (t, u), T0 <= t <= u <= T1, diagonal blocks first.
+    // The rows of a chunk of pixels are copied from the column scratch into
+    // shared memory asynchronously (16-byte cp.async, no registers), one chunk
+    // ahead of the chunk the MMA warps multiply (double buffering); the row
+    // weights k_S, k_L scale the A fragments as the MMA warps read them.
     const int nT = T1 - T0 + 1;
     const int nblk = nT + nT * (nT - 1) / 2;
+    const int SET = CH * NPAD;   // doubles of one row set
     for (int kb = 0; kb < nblk; ++kb) {
       int t, u;
       if (kb < nT) { t = u = T0 + kb; }
@@ -328,11 +355,10 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         while (r >= nT - 1 - tt) { r -= nT - 1 - tt; ++tt; }
         t = T0 + tt; u = t + 1 + r;
       }
-      // warp w < ntile owns tile row w (bp = 8w + lane/4): one accumulator
-      // fragment per tile column (bq = 8c + 2(lane%4) + {0,1})
-      double acc[8][2];
+      const bool diag = t == u;
+      double acc[CC][2];   // tile columns cbeg .. cend-1 of tile row trow
 #pragma unroll
-      for (int c = 0; c < 8; ++c) { acc[c][0] = 0.0; acc[c][1] = 0.0; }
+      for (int c = 0; c < CC; ++c) { acc[c][0] = 0.0; acc[c][1] = 0.0; }
       if (u - t < maxspan) {
         // pixels whose column spans both t and u
         if (tid == 0) s_cnt = 0;
@@ -346,40 +372,61 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         }
         __syncthreads();
         const int n = s_cnt;
-        for (int c0 = 0; c0 < n; c0 += CH) {
-          const int rows = min(CH, n - c0);
-          const int rows4 = (rows + 3) & ~3;   // MMA steps take 4 rows; the padding rows are zero
-          if (tid == 0) n_mma += (unsigned long long)(rows4 / 4) * ntile * ntile * 2;
-          for (int r = warp; r < rows4; r += NW) {   // a warp per staged row, lanes over the bins
-            const double *cs = nullptr, *cl = nullptr;
-            double kS = 0.0, kL = 0.0;
-            int ot = 0, ou = 0;
+        const int nch = (n + CH - 1) / CH;
+        // issue the copies of chunk ci into buffer ci & 1 (rows beyond the
+        // chunk are zeroed with plain stores; columns np .. NPAD-1 stay 0)
+        auto issue = [&](int ci) {
+          double* buf = stage + (size_t)(ci & 1) * 4 * SET;
+          double* kb2 = kbuf + (size_t)(ci & 1) * 2 * CH;
+          const int c0 = ci * CH, rows = min(CH, n - c0), rows4 = (rows + 3) & ~3;
+          const int nset = diag ? 2 : 4;           // a diagonal block reads the rows of t only
+          const int segs = NS / 2;                 // 16-byte segments of a row
+          for (int q = tid; q < nset * rows * segs; q += DT) {
+            const int set = q / (rows * segs), rem = q - set * rows * segs, r = rem / segs, sg = rem - r * segs;
+            const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
+            const int lo = tlo[side * ML + m];
+            const double* colb = (set & 1) ? colL : colS;
+            const int bin = set < 2 ? t : u;
+            const double* src = colb + (size_t)side * ML * TS * NS + ((size_t)m * TS + (bin - lo)) * NS + 2 * sg;
+            __pipeline_memcpy_async(buf + (size_t)set * SET + (size_t)r * NPAD + 2 * sg, src, 16);
+          }
+          for (int q = tid; q < nset * (rows4 - rows) * NPAD; q += DT) {
+            const int set = q / ((rows4 - rows) * NPAD), rem = q - set * (rows4 - rows) * NPAD;
+            buf[(size_t)set * SET + (size_t)rows * NPAD + rem] = 0.0;
+          }
+          for (int r = tid; r < rows4; r += DT) {
+            double ks = 0.0, kl = 0.0;
             if (r < rows) {
               const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
-              const int lo = tlo[side * ML + m];
-              cs = colS + (size_t)side * ML * TS * np + (size_t)m * TS * np;
-              cl = colL + (size_t)side * ML * TS * np + (size_t)m * TS * np;
-              kS = ksc[side * ML + m];
-              kL = klc[side * ML + m];
-              ot = (t - lo) * np;
-              ou = (u - lo) * np;
+              ks = ksc[side * ML + m];
+              kl = klc[side * ML + m];
             }
-            for (int bq = lane; bq < NPAD; bq += 32) {
-              double vs = 0.0, vl = 0.0, us = 0.0, ul = 0.0;
-              if (r < rows && bq < np) {
-                vs = kS * cs[ot + bq];
-                vl = kL * cl[ot + bq];
-                us = cs[ou + bq];
-                ul = cl[ou + bq];
-              }
-              AS[r * NPAD + bq] = vs; AL[r * NPAD + bq] = vl; BS[r * NPAD + bq] = us; BL[r * NPAD + bq] = ul;
-            }
+            kb2[r] = ks;
+            kb2[CH + r] = kl;
           }
-          __syncthreads();
-          if (t == u) {   // moments of bin t from the unscaled rows of the f1 pixels
+          __pipeline_commit();
+        };
+        if (nch > 0) issue(0);
+        for (int ci = 0; ci < nch; ++ci) {
+          if (ci + 1 < nch) {
+            issue(ci + 1);
+            __pipeline_wait_prior(1);   // this thread's copies of chunk ci have landed
+          } else {
+            __pipeline_wait_prior(0);
+          }
+          __syncthreads();               // everyone's copies of chunk ci have landed
+          const double* buf = stage + (size_t)(ci & 1) * 4 * SET;
+          const double* kb2 = kbuf + (size_t)(ci & 1) * 2 * CH;
+          const double* SA = buf;                      // rows of bin t: S, L (unscaled)
+          const double* LA = buf + SET;
+          const double* SB = diag ? SA : buf + 2 * SET;   // rows of bin u
+          const double* LB = diag ? LA : buf + 3 * SET;
+          const int c0 = ci * CH, rows = min(CH, n - c0), rows4 = (rows + 3) & ~3;
+          if (tid == 0) n_mma += (unsigned long long)(rows4 / 4) * ntile * ntile * 2;
+          if (diag) {   // moments of bin t from the rows of the f1 pixels
             for (int e = tid; e < 4 * np; e += DT) {
               const int q = e / np, bq = e - q * np;
-              const double* src = q < 2 ? BS : BL;   // 0: M0, 1: Mi from S; 2: Mj, 3: Mij from L
+              const double* src = q < 2 ? SA : LA;   // 0: M0, 1: Mi from S; 2: Mj, 3: Mij from L
               double sacc = 0.0;
               for (int r = 0; r < rows; ++r) {
                 const int pk = plist[c0 + r];
@@ -391,35 +438,38 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
               mom[(q * nt + t) * np + bq] += sacc;
             }
           }
-          if (warp < ntile) {
+          if (mma_warp) {
             for (int r0 = 0; r0 < rows4; r0 += 4) {
-              const int ra = (r0 + kq) * NPAD;
-              const double as = AS[ra + 8 * warp + grp], al = AL[ra + 8 * warp + grp];
+              const int rr = r0 + kq, ra = rr * NPAD;
+              const double as = SA[ra + 8 * trow + grp] * kb2[rr];
+              const double al = LA[ra + 8 * trow + grp] * kb2[CH + rr];
 #pragma unroll
-              for (int c = 0; c < 8; ++c) {
-                if (c < ntile) {
-                  lya_dmma_8x8x4(acc[c][0], acc[c][1], as, BS[ra + 8 * c + grp]);
-                  lya_dmma_8x8x4(acc[c][0], acc[c][1], al, BL[ra + 8 * c + grp]);
+              for (int c = 0; c < CC; ++c) {
+                const int cc = cbeg + c;
+                if (cc < cend) {
+                  lya_dmma_8x8x4(acc[c][0], acc[c][1], as, SB[ra + 8 * cc + grp]);
+                  lya_dmma_8x8x4(acc[c][0], acc[c][1], al, LB[ra + 8 * cc + grp]);
                 }
               }
             }
           }
-          __syncthreads();
+          __syncthreads();               // buffer ci & 1 is free for chunk ci + 2
         }
       }
-      // flush: column products (subtracted), rank-4 part, diagonal; warp w
-      // writes tile row w, lane (grp, kq) the entries (8w + grp, 8c + 2kq + i)
-      if (warp < ntile) {
-        const int bp = 8 * warp + grp;
+      // flush: column products (subtracted), rank-4 part, diagonal; warp
+      // (trow, thalf) writes the entries (8 trow + grp, 8c + 2kq + i) of its columns
+      if (mma_warp) {
+        const int bp = 8 * trow + grp;
         if (bp < np) {
           const double* mt = mom + (size_t)t * np + bp;   // + q*nt*np
           const double m0a = mt[0], mia = mt[nt * np], mja = mt[2 * nt * np], mija = mt[3 * nt * np];
 #pragma unroll
-          for (int c = 0; c < 8; ++c) {
+          for (int c = 0; c < CC; ++c) {
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-              const int bq = 8 * c + 2 * kq + i;
-              if (c >= ntile || bq >= np) continue;
+              const int cc = cbeg + c;
+              const int bq = 8 * cc + 2 * kq + i;
+              if (cc >= cend || bq >= np) continue;
               const double* mu = mom + (size_t)u * np + bq;
               double v = m0a * mu[0] * cA + mja * mu[2 * nt * np] * cB + mia * mu[nt * np] * cC +
                          mija * mu[3 * nt * np] * cD - acc[c][i];
@@ -503,8 +553,8 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   const int npad = stage_npad(np);
   const int shape = ctx->dist_shape;
   const int DT = DIST_SHAPES[shape].dt, CH = DIST_SHAPES[shape].ch, NW = DT / 32;
-  const size_t stage_len = std::max<size_t>((size_t)4 * CH * npad, (size_t)NW * 2 * TSB * np);
-  const size_t smem = sizeof(double) * (10 * (size_t)max_len + stage_len) +
+  const size_t stage_len = (size_t)stage_doubles(CH, NW, np);
+  const size_t smem = sizeof(double) * (10 * (size_t)max_len + stage_len + 4 * (size_t)CH) +
                       sizeof(int) * (6 * (size_t)max_len);
   if (smem > 227 * 1024)
     return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory (shape %d)",
@@ -519,7 +569,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
     ds = DistScratch{};
     cudaError_t e = lya_alloc(&ds.D, (size_t)nb * nb);
     if (e == cudaSuccess) e = lya_alloc(&ds.W, nb);
-    if (e == cudaSuccess) e = lya_alloc(&ds.col, (size_t)grid * 2 * 2 * max_len * TS * np);
+    if (e == cudaSuccess) e = lya_alloc(&ds.col, (size_t)grid * 2 * 2 * max_len * TS * col_stride(np));
     if (e == cudaSuccess) e = lya_alloc(&ds.mom, (size_t)grid * 4 * nt * np);
     if (e == cudaSuccess) e = lya_alloc(&ds.err, 4);
     if (e != cudaSuccess) {
@@ -543,7 +593,8 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   p.col = ds.col; p.moments = ds.mom; p.D = ds.D; p.W = ds.W; p.err = ds.err; p.next = ds.err + 1;
   p.mma = ds.err + 3;
   p.shape = shape;
-  const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len) + sizeof(int) * (6 * (size_t)ds.max_len);
+  const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len + 4 * (size_t)CH) +
+                          sizeof(int) * (6 * (size_t)ds.max_len);
   static_assert(sizeof(DistParams) <= sizeof(ds.key), "graph key does not fit");
   cudaError_t e = cudaSuccess;
   if (!ds.graph || memcmp(ds.key, &p, sizeof(p)) != 0) {

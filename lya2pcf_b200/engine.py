@@ -291,7 +291,7 @@ class PairEngine:
         self._check(self.lib.lya_dist_run(self.ctx, N.ptr(D), N.ptr(W)))
         return D, W
 
-    DIST_SHAPES = ((512, 32), (512, 16), (512, 64), (256, 32), (256, 16))   # lya_dist_config shapes
+    DIST_SHAPES = ((512, 32), (512, 16), (512, 24), (256, 32), (256, 16))   # lya_dist_config shapes
 
     def autotune_distortion(self, fraction=0.05, min_items=2000):
         """Choose the distortion kernel's launch shape (threads per CTA, pixels
