@@ -30,6 +30,8 @@
  *                      correlation_procedures_cpu.py:46-84 (ra/dec angle with the
  *                      2-arcsec small-angle branch, the dtheta < angmax cut and
  *                      int(r/rmax*n) truncation).
+ *   orc_corr_wdw       the reference kernel's own work only (W and DW with the
+ *                      formula of orc_corr): the timed CPU baseline.
  *   orc_adjoint        gradient of L = sum_b g_b * DW_b/W_b (no reference code):
  *                      for each in-range pair in bin b,
  *                        dL/ddw_i += (g_b/W_b) dw_j,  dL/ddw_j += (g_b/W_b) dw_i,
@@ -387,6 +389,61 @@ int orc_corr(const orc_forests* F, int64_t nslot, const int64_t* slot_item_start
   c.rpmax = rpmax; c.rtmax = rtmax; c.np = np; c.nt = nt; c.mode = mode; c.cos_variant = cos_variant;
   c.angmax = angmax; c.out = out; c.cnt = cnt;
   pool_run(nthreads, nslot, corr_task, &c);
+  return 0;
+}
+
+/* ------------------------------------------------------------ baseline timing */
+/* The reference kernel's own work only (cuda_kernels.cpp:118-159): W and DW of
+ * every pixel pair of the listed forest pairs with the FP64 formula of
+ * orc_corr (contraction 0), per slot, out[nslot][2][np*nt] accumulated into.
+ * Used to time the CPU baseline: no extra outputs, threads over slots. */
+typedef struct {
+  const orc_forests* F;
+  const int32_t *f1, *f2;
+  const int64_t* sis;
+  double binner_rp, binner_rt;
+  int np, nt;
+  double* out;
+} wdw_ctx;
+
+static void wdw_task(void* vctx, int64_t slot) {
+  const wdw_ctx* c = (const wdw_ctx*)vctx;
+  const orc_forests* F = c->F;
+  const int nb = c->np * c->nt;
+  double* hw = c->out + (size_t)slot * 2 * nb;
+  double* hd = hw + nb;
+  const double fnp = (double)c->np, fnt = (double)c->nt;
+  for (int64_t it = c->sis[slot]; it < c->sis[slot + 1]; ++it) {
+    const int64_t a = c->f1[it], b = c->f2[it];
+    const int64_t s1 = F->start[a], l1 = F->start[a + 1] - s1;
+    const int64_t s2 = F->start[b], l2 = F->start[b + 1] - s2;
+    const double cos12 = cos12_clamped(F->ux[a], F->uy[a], F->uz[a], F->ux[b], F->uy[b], F->uz[b], 0);
+    const double chh = sqrt(0.5 * (1. + cos12)), shh = sqrt(0.5 * (1. - cos12));
+    const double* d2 = F->dc + s2;
+    const double* w2 = F->w + s2;
+    const double* dw2 = F->dw + s2;
+    for (int64_t i = 0; i < l1; ++i) {
+      const double d1 = F->dc[s1 + i], w1 = F->w[s1 + i], dw1 = F->dw[s1 + i];
+      for (int64_t j = 0; j < l2; ++j) {
+        const double fp = floor(fabs(d1 - d2[j]) * chh * c->binner_rp);
+        const double ft = floor((d1 + d2[j]) * shh * c->binner_rt);
+        if (fp >= 0.0 && fp < fnp && ft >= 0.0 && ft < fnt) {
+          const int k = (int)fp * c->nt + (int)ft;
+          hw[k] += w1 * w2[j];
+          hd[k] += dw1 * dw2[j];
+        }
+      }
+    }
+  }
+}
+
+int orc_corr_wdw(const orc_forests* F, int64_t nslot, const int64_t* slot_item_start, const int32_t* f1,
+                 const int32_t* f2, double rpmax, double rtmax, int np, int nt, double* out, int nthreads) {
+  wdw_ctx c;
+  c.F = F; c.f1 = f1; c.f2 = f2; c.sis = slot_item_start;
+  c.binner_rp = (double)np / rpmax; c.binner_rt = (double)nt / rtmax;
+  c.np = np; c.nt = nt; c.out = out;
+  pool_run(nthreads, nslot, wdw_task, &c);
   return 0;
 }
 

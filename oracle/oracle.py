@@ -42,6 +42,7 @@ def lib():
         L.orc_neighbours.argtypes = [P, P, P, C.c_double, C.c_double, P, P, P, C.c_int]
         L.orc_corr.argtypes = [P, C.c_int64, P, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                C.c_double, P, P, C.c_int]
+        L.orc_corr_wdw.argtypes = [P, C.c_int64, P, P, P, C.c_double, C.c_double, C.c_int, C.c_int, P, C.c_int]
         L.orc_adjoint.argtypes = [P, C.c_int64, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, P, P, P, P]
         L.orc_distortion.argtypes = [P, C.c_int64, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, P, P]
         L.orc_distortion_mode.argtypes = [P, C.c_int64, P, P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
@@ -50,7 +51,7 @@ def lib():
                                     C.c_int, P, P]
         L.orc_cos12.argtypes = [C.c_double] * 6 + [C.c_int]
         L.orc_cos12.restype = C.c_double
-        for f in ('orc_neighbours', 'orc_corr', 'orc_adjoint', 'orc_distortion', 'orc_distortion_mode',
+        for f in ('orc_neighbours', 'orc_corr', 'orc_corr_wdw', 'orc_adjoint', 'orc_distortion', 'orc_distortion_mode',
                   'orc_dist_bins'):
             getattr(L, f).restype = C.c_int
         _lib = L
@@ -152,6 +153,22 @@ def corr(fs, f1, f2, slot_item_start, rpmax=200.0, rtmax=200.0, np_=50, nt=50, m
                         int(mode), int(cos_variant), float(angmax), _ptr(out), _ptr(cnt), int(nthreads))
     assert rc == 0
     return out, cnt
+
+
+def corr_wdw(fs, f1, f2, slot_item_start, rpmax=200.0, rtmax=200.0, np_=50, nt=50, nthreads=None, cat=None):
+    """W and DW only (the reference kernel's outputs), ``out[nslot, 2, np*nt]``:
+    the work the CPU baseline times."""
+    cat = cat or Catalog(fs)
+    nthreads = nthreads or os.cpu_count() or 1
+    nslot = len(slot_item_start) - 1
+    out = np.zeros((nslot, 2, np_ * nt), dtype=np.float64)
+    f1 = np.ascontiguousarray(f1, dtype=np.int32)
+    f2 = np.ascontiguousarray(f2, dtype=np.int32)
+    sis = np.ascontiguousarray(slot_item_start, dtype=np.int64)
+    rc = lib().orc_corr_wdw(cat.ref, nslot, _ptr(sis), _ptr(f1), _ptr(f2), float(rpmax), float(rtmax), int(np_),
+                            int(nt), _ptr(out), int(nthreads))
+    assert rc == 0
+    return out
 
 
 def adjoint(fs, f1, f2, coef_dw, coef_w, rpmax=200.0, rtmax=200.0, np_=50, nt=50, cos_variant=0, cat=None):

@@ -254,3 +254,15 @@ def test_distortion_fp32_binning_differs_only_through_bins():
     D32, W32 = O.distortion(fs, f1, f2, bin_mode=O.BIN_FP32)
     assert W64.sum() > 0 and not np.array_equal(W32, W64)
     np.testing.assert_allclose(W32.sum(), W64.sum(), rtol=1e-2)
+
+
+def test_wdw_baseline_equals_full_oracle():
+    """The W/DW-only path the CPU baseline times gives the full oracle's W and
+    DW bit for bit."""
+    from lya2pcf_b200 import synthetic
+    fs = synthetic.make(0, scale=0.05)
+    off, nbr = O.neighbours(fs, synthetic.angmax_for(fs))
+    f1, f2, sis, _ = O.items_from_csr(fs, off, nbr)
+    h, _ = O.corr(fs, f1, f2, sis)
+    w = O.corr_wdw(fs, f1, f2, sis)
+    assert np.array_equal(w[:, 0], h[:, O.Q_W]) and np.array_equal(w[:, 1], h[:, O.Q_DW])
