@@ -367,13 +367,18 @@ def run_b200(args, dist):
     if not args.no_covariance:
         try:
             t = time.perf_counter()
+            eng.covariance()
+            first_s = time.perf_counter() - t
+            t = time.perf_counter()
             mean, cmat, csm, smoothed = eng.covariance()
             cov_s = time.perf_counter() - t
-            covariance = {'seconds': cov_s, 'gram_kernels_ms': eng.stats()['kernel_ms'], 'rows': len(slot_pixels),
+            covariance = {'seconds': cov_s, 'first_call_seconds': first_s,
+                          'gram_kernels_ms': eng.stats()['kernel_ms'], 'rows': len(slot_pixels),
                           'bins': eng.nb, 'smoothed': smoothed,
                           'gram_fma': float(len(slot_pixels)) * eng.nb * eng.nb,
                           'what': 'lya_covariance (rows from the run on the device, FP64 tensor-core Gram) + '
-                                  'lya_covariance_smooth, wall clock with the 50 MB copies out'}
+                                  'lya_covariance_smooth, wall clock with the 50 MB copies out (second call; '
+                                  'the first, with its host and device allocations, in first_call_seconds)'}
         except N.LyaError as err:
             covariance = {'error': str(err)}
 
