@@ -115,6 +115,29 @@ __device__ __forceinline__ double pair_ft(double d1, double d2, double sh, const
   return floor(__dmul_rn(__dmul_rn(__dadd_rn(d1, d2), sh), p.binner_rt));
 }
 
+// First index in [lo, hi) of the sorted shared array a at which the monotone
+// predicate holds (hi when it holds nowhere), found by the whole warp: 32
+// probes and one vote per level, ceil(log32(hi - lo)) + 1 levels instead of
+// log2(hi - lo) dependent steps of a binary search.
+template <class Pred>
+__device__ __forceinline__ int warp_first(const double* a, int lo, int hi, Pred pred) {
+  const int lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const int step = (hi - lo + 31) >> 5;
+    const int idx = lo + (lane + 1) * step - 1;
+    const bool t = lane == 31 || idx >= hi || pred(a[idx]);   // the last lane closes the range
+    const unsigned bal = __ballot_sync(0xffffffffu, t);
+    const int f = __ffs(bal) - 1;
+    const int pf = lo + (f + 1) * step - 1;     // lane f's probe (true, or the closing lane)
+    const int nhi = (f == 31 || pf >= hi) ? hi : pf;
+    lo += f * step;                             // lane f-1's probe was false
+    hi = nhi;
+  }
+  const int idx = lo + lane;
+  const unsigned bal = __ballot_sync(0xffffffffu, idx < hi && pred(a[idx]));
+  return bal ? lo + __ffs(bal) - 1 : hi;
+}
+
 template <int DT, int CH>
 __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   constexpr int NW = DT / 32;   // warps per CTA
@@ -206,12 +229,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           const double rt_reach = sh > 0.0 ? ((double)nt + 1e-3) / (sh * p.binner_rt) : 1e300;
           const double tl = d - reach - 1e-6 * fabs(d) - 1e-6;
           const double th = fmin(d + reach, rt_reach - d) + 1e-6 * fabs(d) + 1e-6;
-          int x = 0, y = Lo;
-          while (x < y) { const int q = (x + y) >> 1; if (dO[q] > tl) y = q; else x = q + 1; }
-          jlo = x;
-          y = Lo;
-          while (x < y) { const int q = (x + y) >> 1; if (dO[q] < th) x = q + 1; else y = q; }
-          jhi = x;
+          jlo = warp_first(dO, 0, Lo, [&](double v) { return v > tl; });
+          jhi = warp_first(dO, jlo, Lo, [&](double v) { return !(v < th); });
         }
         // window of rt bins the column can touch, and the built rows
         int wlo = 0, nrow = 0;
@@ -242,9 +261,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             const int je = min(jhi, j + seg);
             int cbp = -1, cbt = -1;
             double as = 0.0, al = 0.0;
-            for (; j < je; ++j) {
-              int bp, bt;
-              const bool in = side == 0 ? pair_bin2(d, dO[j], ch, sh, p, bp, bt) : pair_bin2(dO[j], d, ch, sh, p, bp, bt);
+            auto merge = [&](bool in, int bp, int bt, double wj, double lj) {
               if (!in) { bp = -1; bt = -1; }
               if (bp != cbp || bt != cbt) {
                 if (cbp >= 0) {
@@ -255,11 +272,32 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
                 cbp = bp; cbt = bt; as = 0.0; al = 0.0;
               }
               if (in) {
-                as += wO[j];
-                al = fma(wO[j], lO[j], al);
+                as += wj;
+                al = fma(wj, lj, al);
                 lo = min(lo, bt);
                 hi = max(hi, bt);
               }
+            };
+            // bins of four partners at a time (independent FP64 chains), then
+            // the runs in partner order
+            for (; j + 4 <= je; j += 4) {
+              int bp[4], bt[4];
+              bool in[4];
+              double wj[4], lj[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const double dj = dO[j + u];
+                wj[u] = wO[j + u];
+                lj[u] = lO[j + u];
+                in[u] = side == 0 ? pair_bin2(d, dj, ch, sh, p, bp[u], bt[u]) : pair_bin2(dj, d, ch, sh, p, bp[u], bt[u]);
+              }
+#pragma unroll
+              for (int u = 0; u < 4; ++u) merge(in[u], bp[u], bt[u], wj[u], lj[u]);
+            }
+            for (; j < je; ++j) {
+              int bp, bt;
+              const bool in = side == 0 ? pair_bin2(d, dO[j], ch, sh, p, bp, bt) : pair_bin2(dO[j], d, ch, sh, p, bp, bt);
+              merge(in, bp, bt, wO[j], lO[j]);
             }
             if (cbp >= 0) {
               const int q = (cbt - wlo) * np + cbp;
@@ -313,10 +351,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           double* rs = cS + (size_t)m * TS * NS;
           double* rl = cL + (size_t)m * TS * NS;
           const int off = (lo - wlo) * np;
-          for (int q = lane; q < sp * NS; q += 32) {
-            const int row = q / NS, col = q - row * NS;
-            rs[q] = col < np ? myS[off + row * np + col] : 0.0;
-            rl[q] = col < np ? myL[off + row * np + col] : 0.0;
+          for (int row = 0; row < sp; ++row) {
+            for (int col = lane; col < NS; col += 32) {
+              rs[row * NS + col] = col < np ? myS[off + row * np + col] : 0.0;
+              rl[row * NS + col] = col < np ? myL[off + row * np + col] : 0.0;
+            }
           }
           if (lane == 0) {
             atomicMin(&s_T0, lo);
