@@ -30,8 +30,9 @@
 // from the same staged rows).  A block whose rt bins are both spanned by some
 // pixel column gets the column products as a small dense FP64 GEMM on the
 // tensor cores: the rows of the pixels covering t and u are staged in shared
-// memory in chunks of CH pixels, and warp w accumulates tile row w of the
-// block (8 x 8 tiles, mma.sync m8n8k4 f64; FP64 has no tcgen05 kind); the
+// memory in chunks of CH pixels, and each warp accumulates 16 x 8 tiles of the
+// block (four tiles of 16 rp bins down, 8 across; mma.sync m16n8k8 f64, FP64
+// having no tcgen05 kind; rows at or beyond np enter as zeros); the
 // rank-4 and diagonal terms are added to the accumulators, and each D entry of
 // the window gets one atomic add per forest pair (both (A, B) and (B, A): D is
 // symmetric).
@@ -49,9 +50,9 @@ namespace {
 
 constexpr int TS = 8;         // rt bins a pixel column may span
 constexpr int TSB = TS + 2;   // rows of a column being built (its window may be one bin wider at each end)
-constexpr int NP_MAX = 64;    // np of the blocks: at most 8 x 8 tiles of 8 x 8
+constexpr int NP_MAX = 64;    // np of the blocks: at most 4 x 8 tiles of 16 x 8
 // Launch shapes the autotuner chooses from: threads per CTA (DT) and pixels per
-// staged chunk of a block (CH, a multiple of 4).  Shape 0 is the default.
+// staged chunk of a block (CH, a multiple of 8: the K of one MMA).  Shape 0 is the default.
 struct DistShape { int dt, ch; };
 constexpr DistShape DIST_SHAPES[] = {{512, 32}, {512, 16}, {512, 24}, {256, 32}, {256, 16}};
 constexpr int N_DIST_SHAPES = sizeof(DIST_SHAPES) / sizeof(DIST_SHAPES[0]);
@@ -92,7 +93,7 @@ struct DistParams {
   double* W;               // [nb]
   unsigned long long* err; // [1] pixels whose column spans more than TS rt bins
   unsigned long long* next;// [1] work queue counter
-  unsigned long long* mma; // [1] FP64 tensor-core MMAs (m8n8k4) issued, for the roofline
+  unsigned long long* mma; // [1] block-product work in m8n8k4 units (8x8 tiles, rows rounded to 4), for the roofline
   int shape;               // launch shape (DIST_SHAPES index); part of the captured graph's key
 };
 
@@ -141,9 +142,9 @@ __device__ __forceinline__ int warp_first(const double* a, int lo, int hi, Pred 
 template <int DT, int CH>
 __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   constexpr int NW = DT / 32;   // warps per CTA
-  // accumulator fragments per MMA warp: with 16 warps or more, two warps share a
-  // tile row (np <= 64: at most 8 tile columns, 4 each); otherwise one warp per row
-  constexpr int CC = NW >= 16 ? 4 : 8;
+  // 16 x 8 accumulator tiles per warp: NW/4 warps share each of the four tile
+  // rows of 16 rp bins (np <= 64), and split its (at most 8) tile columns
+  constexpr int CC = NW >= 16 ? 2 : 4;
   extern __shared__ __align__(16) unsigned char smem[];
   const int ML = p.max_len;
   const int np = p.np, nt = p.nt, nb = p.nb, NPAD = p.npad;
@@ -169,12 +170,10 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   double* myS = stage + (size_t)warp * 2 * TSB * np;
   double* myL = myS + TSB * np;
   const int ntile = (np + 7) / 8;   // tile rows = tile columns of a 50x50 block (7 for np = 50)
-  // MMA warps: tile row (w mod ntile) and, with two warps per tile row, one
-  // half of the tile columns each
-  const int nsplit = CC == 4 ? 2 : 1;
-  const int trow = warp % ntile, thalf = warp / ntile;
-  const int ccols = (ntile + nsplit - 1) / nsplit, cbeg = thalf * ccols, cend = min(ntile, cbeg + ccols);
-  const bool mma_warp = warp < ntile * nsplit;
+  // warp w: tile row mt = w mod 4 (rp bins 16 mt .. 16 mt + 15) and tile
+  // columns ng, ng + nwm, ... (ng = w / 4) of 8 rp bins each
+  const int nwm = NW / 4;
+  const int mt = warp & 3, ng = warp >> 2;
   const int grp = lane >> 2, kq = lane & 3;
   unsigned long long n_mma = 0;     // thread 0: MMAs of this CTA
 
@@ -395,9 +394,9 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         t = T0 + tt; u = t + 1 + r;
       }
       const bool diag = t == u;
-      double acc[CC][2];   // tile columns cbeg .. cend-1 of tile row trow
+      double acc[CC][4];
 #pragma unroll
-      for (int c = 0; c < CC; ++c) { acc[c][0] = 0.0; acc[c][1] = 0.0; }
+      for (int c = 0; c < CC; ++c) { acc[c][0] = 0.0; acc[c][1] = 0.0; acc[c][2] = 0.0; acc[c][3] = 0.0; }
       if (u - t < maxspan) {
         // pixels whose column spans both t and u
         if (tid == 0) s_cnt = 0;
@@ -417,7 +416,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         auto issue = [&](int ci) {
           double* buf = stage + (size_t)(ci & 1) * 4 * SET;
           double* kb2 = kbuf + (size_t)(ci & 1) * 2 * CH;
-          const int c0 = ci * CH, rows = min(CH, n - c0), rows4 = (rows + 3) & ~3;
+          const int c0 = ci * CH, rows = min(CH, n - c0), rows8 = (rows + 7) & ~7;
           const int nset = diag ? 2 : 4;           // a diagonal block reads the rows of t only
           const int segs = NS / 2;                 // 16-byte segments of a row
           for (int q = tid; q < nset * rows * segs; q += DT) {
@@ -429,11 +428,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             const double* src = colb + (size_t)side * ML * TS * NS + ((size_t)m * TS + (bin - lo)) * NS + 2 * sg;
             __pipeline_memcpy_async(buf + (size_t)set * SET + (size_t)r * NPAD + 2 * sg, src, 16);
           }
-          for (int q = tid; q < nset * (rows4 - rows) * NPAD; q += DT) {
-            const int set = q / ((rows4 - rows) * NPAD), rem = q - set * (rows4 - rows) * NPAD;
+          for (int q = tid; q < nset * (rows8 - rows) * NPAD; q += DT) {
+            const int set = q / ((rows8 - rows) * NPAD), rem = q - set * (rows8 - rows) * NPAD;
             buf[(size_t)set * SET + (size_t)rows * NPAD + rem] = 0.0;
           }
-          for (int r = tid; r < rows4; r += DT) {
+          for (int r = tid; r < rows8; r += DT) {
             double ks = 0.0, kl = 0.0;
             if (r < rows) {
               const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
@@ -460,8 +459,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           const double* LA = buf + SET;
           const double* SB = diag ? SA : buf + 2 * SET;   // rows of bin u
           const double* LB = diag ? LA : buf + 3 * SET;
-          const int c0 = ci * CH, rows = min(CH, n - c0), rows4 = (rows + 3) & ~3;
-          if (tid == 0) n_mma += (unsigned long long)(rows4 / 4) * ntile * ntile * 2;
+          const int c0 = ci * CH, rows = min(CH, n - c0), rows8 = (rows + 7) & ~7;
+          if (tid == 0) n_mma += (unsigned long long)((rows + 3) / 4) * ntile * ntile * 2;
           if (diag) {   // moments of bin t from the rows of the f1 pixels
             for (int e = tid; e < 4 * np; e += DT) {
               const int q = e / np, bq = e - q * np;
@@ -477,17 +476,23 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
               mom[(q * nt + t) * np + bq] += sacc;
             }
           }
-          if (mma_warp) {
-            for (int r0 = 0; r0 < rows4; r0 += 4) {
-              const int rr = r0 + kq, ra = rr * NPAD;
-              const double as = SA[ra + 8 * trow + grp] * kb2[rr];
-              const double al = LA[ra + 8 * trow + grp] * kb2[CH + rr];
+          {
+            const int bp0 = 16 * mt + grp, bp1 = bp0 + 8;
+            const bool v0 = bp0 < np, v1 = bp1 < np;
+            for (int r0 = 0; r0 < rows8; r0 += 8) {
+              const int ra = (r0 + kq) * NPAD, rb = ra + 4 * NPAD;
+              const double ks0 = kb2[r0 + kq], ks1 = kb2[r0 + kq + 4];
+              const double kl0 = kb2[CH + r0 + kq], kl1 = kb2[CH + r0 + kq + 4];
+              const double as0 = v0 ? SA[ra + bp0] * ks0 : 0.0, as1 = v1 ? SA[ra + bp1] * ks0 : 0.0;
+              const double as2 = v0 ? SA[rb + bp0] * ks1 : 0.0, as3 = v1 ? SA[rb + bp1] * ks1 : 0.0;
+              const double al0 = v0 ? LA[ra + bp0] * kl0 : 0.0, al1 = v1 ? LA[ra + bp1] * kl0 : 0.0;
+              const double al2 = v0 ? LA[rb + bp0] * kl1 : 0.0, al3 = v1 ? LA[rb + bp1] * kl1 : 0.0;
 #pragma unroll
               for (int c = 0; c < CC; ++c) {
-                const int cc = cbeg + c;
-                if (cc < cend) {
-                  lya_dmma_8x8x4(acc[c][0], acc[c][1], as, SB[ra + 8 * cc + grp]);
-                  lya_dmma_8x8x4(acc[c][0], acc[c][1], al, LB[ra + 8 * cc + grp]);
+                const int nt8 = ng + nwm * c;
+                if (nt8 < ntile) {
+                  lya_dmma_16x8x8(acc[c], as0, as1, as2, as3, SB[ra + 8 * nt8 + grp], SB[rb + 8 * nt8 + grp]);
+                  lya_dmma_16x8x8(acc[c], al0, al1, al2, al3, LB[ra + 8 * nt8 + grp], LB[rb + 8 * nt8 + grp]);
                 }
               }
             }
@@ -497,21 +502,22 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
       }
       // flush: column products (subtracted), rank-4 part, diagonal; warp
       // (trow, thalf) writes the entries (8 trow + grp, 8c + 2kq + i) of its columns
-      if (mma_warp) {
-        const int bp = 8 * trow + grp;
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        const int bp = 16 * mt + grp + 8 * h2;
         if (bp < np) {
-          const double* mt = mom + (size_t)t * np + bp;   // + q*nt*np
-          const double m0a = mt[0], mia = mt[nt * np], mja = mt[2 * nt * np], mija = mt[3 * nt * np];
+          const double* mtp = mom + (size_t)t * np + bp;   // + q*nt*np
+          const double m0a = mtp[0], mia = mtp[nt * np], mja = mtp[2 * nt * np], mija = mtp[3 * nt * np];
 #pragma unroll
           for (int c = 0; c < CC; ++c) {
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-              const int cc = cbeg + c;
-              const int bq = 8 * cc + 2 * kq + i;
-              if (cc >= cend || bq >= np) continue;
+              const int nt8 = ng + nwm * c;
+              const int bq = 8 * nt8 + 2 * kq + i;
+              if (nt8 >= ntile || bq >= np) continue;
               const double* mu = mom + (size_t)u * np + bq;
               double v = m0a * mu[0] * cA + mja * mu[2 * nt * np] * cB + mia * mu[nt * np] * cC +
-                         mija * mu[3 * nt * np] * cD - acc[c][i];
+                         mija * mu[3 * nt * np] * cD - acc[c][2 * h2 + i];
               const int A = bp * nt + t, B = bq * nt + u;
               if (A == B) {
                 v += m0a;
@@ -563,6 +569,9 @@ cudaError_t launch_dist(int shape, int grid, size_t smem, cudaStream_t s, const 
   }
 }
 static_assert(N_DIST_SHAPES == 5, "the launch tables above cover every shape");
+static_assert(DIST_SHAPES[0].ch % 8 == 0 && DIST_SHAPES[1].ch % 8 == 0 && DIST_SHAPES[2].ch % 8 == 0 &&
+                  DIST_SHAPES[3].ch % 8 == 0 && DIST_SHAPES[4].ch % 8 == 0 && DIST_SHAPES[3].dt % 128 == 0,
+              "chunks hold whole MMA K steps; the warps cover the four tile rows");
 
 }  // namespace
 

@@ -270,6 +270,18 @@ __device__ __forceinline__ void lya_dmma_8x8x4(double& d0, double& d1, double a,
                : "d"(a), "d"(b));
 }
 
+// FP64 tensor-core MMA, D (16x8) += A (16x8, row-major) x B (8x8, column-major).
+// Fragments, with g = lane / 4 and q = lane % 4: a0 (g, q), a1 (g+8, q),
+// a2 (g, q+4), a3 (g+8, q+4); b0 (q, g), b1 (q+4, g); c0, c1 (g, 2q and 2q+1),
+// c2, c3 (g+8, 2q and 2q+1).  Four times the work of one m8n8k4 per instruction.
+__device__ __forceinline__ void lya_dmma_16x8x8(double (&c)[4], double a0, double a1, double a2, double a3,
+                                                double b0, double b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+               "{%0, %1, %2, %3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 // ------------------------------------------------------------------ launchers
 int lya_corr_launch(lya_ctx* ctx, const lya_corr_opts* o);
 int lya_build_queue(lya_ctx* ctx, double angmax, double mumin);
