@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   double* mom = p.moments + (size_t)blockIdx.x * 4 * nt * np;   // [4][nt][np] (CTA-private, L2-resident)
   double* stage = klc + 2 * ML;                          // 2 x [4][CH][NPAD] staged rows, or the column builders
   const int stage_len = stage_doubles(CH, NW, np);
-  double* kbuf = stage + stage_len;                      // [2][2][CH] per staged row: k_S, k_L
-  int* tlo = reinterpret_cast<int*>(kbuf + 4 * CH);      // [2][ML]
+  double* kbuf = stage + stage_len;                      // [2][4][CH] per staged row: k_S, k_L, f1 w, f1 w dl
+  int* tlo = reinterpret_cast<int*>(kbuf + 8 * CH);      // [2][ML]
   int* span = tlo + 2 * ML;                              // [2][ML]
   int* plist = span + 2 * ML;                            // [2*ML] packed (side << 16 | pixel)
   __shared__ int s_T0, s_T1, s_maxspan, s_cnt;
@@ -165,6 +165,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int NS = col_stride(np);
+  // q / (NS/2) as a multiply-high: exact for q < 2^16 (the copies of a chunk)
+  const unsigned seg_magic = (unsigned)((0x100000000ull + (unsigned)(NS / 2) - 1) / (unsigned)(NS / 2));
   double* colS = p.col + (size_t)blockIdx.x * 2 * 2 * ML * TS * NS;   // [2 sides][ML][TS][NS]
   double* colL = colS + (size_t)2 * ML * TS * NS;
   double* myS = stage + (size_t)warp * 2 * TSB * np;
@@ -415,12 +417,15 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         // chunk are zeroed with plain stores; columns np .. NPAD-1 stay 0)
         auto issue = [&](int ci) {
           double* buf = stage + (size_t)(ci & 1) * 4 * SET;
-          double* kb2 = kbuf + (size_t)(ci & 1) * 2 * CH;
+          double* kb2 = kbuf + (size_t)(ci & 1) * 4 * CH;
           const int c0 = ci * CH, rows = min(CH, n - c0), rows8 = (rows + 7) & ~7;
           const int nset = diag ? 2 : 4;           // a diagonal block reads the rows of t only
           const int segs = NS / 2;                 // 16-byte segments of a row
-          for (int q = tid; q < nset * rows * segs; q += DT) {
-            const int set = q / (rows * segs), rem = q - set * rows * segs, r = rem / segs, sg = rem - r * segs;
+          // q = (set CH + r) segs + sg over whole chunks; rows r >= rows are skipped
+          for (int q = tid; q < nset * CH * segs; q += DT) {
+            const int sr = (int)__umulhi((unsigned)q, seg_magic), sg = q - sr * segs;
+            const int set = sr / CH, r = sr - set * CH;
+            if (r >= rows) continue;
             const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
             const int lo = tlo[side * ML + m];
             const double* colb = (set & 1) ? colL : colS;
@@ -433,14 +438,17 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             buf[(size_t)set * SET + (size_t)rows * NPAD + rem] = 0.0;
           }
           for (int r = tid; r < rows8; r += DT) {
-            double ks = 0.0, kl = 0.0;
+            double ks = 0.0, kl = 0.0, w0 = 0.0, w1 = 0.0;
             if (r < rows) {
               const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
               ks = ksc[side * ML + m];
               kl = klc[side * ML + m];
+              if (side == 0) { w0 = sw[m]; w1 = sw[m] * sl[m]; }
             }
             kb2[r] = ks;
             kb2[CH + r] = kl;
+            kb2[2 * CH + r] = w0;
+            kb2[3 * CH + r] = w1;
           }
           __pipeline_commit();
         };
@@ -454,7 +462,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           }
           __syncthreads();               // everyone's copies of chunk ci have landed
           const double* buf = stage + (size_t)(ci & 1) * 4 * SET;
-          const double* kb2 = kbuf + (size_t)(ci & 1) * 2 * CH;
+          const double* kb2 = kbuf + (size_t)(ci & 1) * 4 * CH;
           const double* SA = buf;                      // rows of bin t: S, L (unscaled)
           const double* LA = buf + SET;
           const double* SB = diag ? SA : buf + 2 * SET;   // rows of bin u
@@ -464,15 +472,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           if (diag) {   // moments of bin t from the rows of the f1 pixels
             for (int e = tid; e < 4 * np; e += DT) {
               const int q = e / np, bq = e - q * np;
-              const double* src = q < 2 ? SA : LA;   // 0: M0, 1: Mi from S; 2: Mj, 3: Mij from L
+              const double* src = (q < 2 ? SA : LA) + bq;   // 0: M0, 1: Mi from S; 2: Mj, 3: Mij from L
+              const double* cw = kb2 + ((q == 0 || q == 2) ? 2 : 3) * CH;   // f1 w or w dl, 0 for f2 rows
               double sacc = 0.0;
-              for (int r = 0; r < rows; ++r) {
-                const int pk = plist[c0 + r];
-                if ((pk >> 16) != 0) continue;
-                const int m = pk & 0xffff;
-                const double cw = (q == 0 || q == 2) ? sw[m] : sw[m] * sl[m];
-                sacc += cw * src[r * NPAD + bq];
-              }
+#pragma unroll 4
+              for (int r = 0; r < rows; ++r) sacc = fma(cw[r], src[r * NPAD], sacc);
               mom[(q * nt + t) * np + bq] += sacc;
             }
           }
@@ -602,7 +606,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   const int shape = ctx->dist_shape;
   const int DT = DIST_SHAPES[shape].dt, CH = DIST_SHAPES[shape].ch, NW = DT / 32;
   const size_t stage_len = (size_t)stage_doubles(CH, NW, np);
-  const size_t smem = sizeof(double) * (10 * (size_t)max_len + stage_len + 4 * (size_t)CH) +
+  const size_t smem = sizeof(double) * (10 * (size_t)max_len + stage_len + 8 * (size_t)CH) +
                       sizeof(int) * (6 * (size_t)max_len);
   if (smem > 227 * 1024)
     return lya_fail(ctx, LYA_ERR_DATA, "lya_dist_run: forests of %d pixels need %zu B of shared memory (shape %d)",
@@ -641,7 +645,7 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   p.col = ds.col; p.moments = ds.mom; p.D = ds.D; p.W = ds.W; p.err = ds.err; p.next = ds.err + 1;
   p.mma = ds.err + 3;
   p.shape = shape;
-  const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len + 4 * (size_t)CH) +
+  const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len + 8 * (size_t)CH) +
                           sizeof(int) * (6 * (size_t)ds.max_len);
   static_assert(sizeof(DistParams) <= sizeof(ds.key), "graph key does not fit");
   cudaError_t e = cudaSuccess;
