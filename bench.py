@@ -513,7 +513,8 @@ def distortion_sample(scale, dev):
                          'peak': DMMA_PEAK_TFLOPS, 'frac': flops / (ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS,
                          'flops': flops,
                          'peak_source': 'nominal B200 FP64 tensor-core rate (data sheet, not measured)',
-                         'what': 'm8n8k4 FP64 MMAs of the column block products (counted by the kernel)'}}
+                         'what': 'flops of the column block products (8x8 tiles over the staged rows, counted '
+                                 'by the kernel; run as m16n8k8 FP64 MMAs)'}}
 
 
 XI_FLOOR_FRAC = 0.1   # per-bin xi errors are stated over bins with |xi| >= this fraction of the median |xi|

@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             const int set = q / ((rows8 - rows) * NPAD), rem = q - set * (rows8 - rows) * NPAD;
             buf[(size_t)set * SET + (size_t)rows * NPAD + rem] = 0.0;
           }
-          for (int r = tid; r < rows8; r += DT) {
+          for (int r = tid - (DT - 32); r >= 0 && r < rows8; r += 32) {   // the last warp
             double ks = 0.0, kl = 0.0, w0 = 0.0, w1 = 0.0;
             if (r < rows) {
               const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
