@@ -27,7 +27,10 @@
 // its partners) go to CTA-private global scratch as dense [TS rt bins][np]
 // rows.  Phase 2: the 50x50 (rp x rp) blocks (t, u) of D over the pair's window
 // of rt bins, diagonal blocks first (they complete the moments of bin t, read
-// from the same staged rows).  A block whose rt bins are both spanned by some
+// from the same staged rows: the f1 weights placed in padding columns
+// NS..NS+3 of the staged rows make accumulator rows NS..NS+3 of the diagonal
+// block's MMAs the four moments, when NS + 4 <= 64; otherwise a loop over the
+// staged rows).  A block whose rt bins are both spanned by some
 // pixel column gets the column products as a small dense FP64 GEMM on the
 // tensor cores: the rows of the pixels covering t and u are staged in shared
 // memory in chunks of CH pixels, and each warp accumulates 16 x 8 tiles of the
@@ -192,6 +195,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
     const double ch = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(1.0, c)));
     const double sh = __dsqrt_rn(__dmul_rn(0.5, __dsub_rn(1.0, c)));
     const double om1 = p.omega[a], om2 = p.omega[b];
+    const double odl2b = p.odl2[b];
     const double io1 = p.odl2[a] > 0.0 ? 1.0 / p.odl2[a] : 0.0;
     const double io2 = p.odl2[b] > 0.0 ? 1.0 / p.odl2[b] : 0.0;
     const bool srt = p.sorted[a] && p.sorted[b];
@@ -449,6 +453,19 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             kb2[CH + r] = kl;
             kb2[2 * CH + r] = w0;
             kb2[3 * CH + r] = w1;
+            if (diag && NS + 4 <= 64) {   // moment columns of the S and L rows of bin t
+              double dlm = 0.0;
+              bool f1r = false;
+              if (r < rows) {
+                const int pk = plist[c0 + r];
+                f1r = (pk >> 16) == 0;
+                dlm = sl[pk & 0xffff];
+              }
+              double* rs = buf + (size_t)r * NPAD + NS;
+              double* rl = buf + SET + (size_t)r * NPAD + NS;
+              rs[0] = f1r ? om2 : 0.0; rs[1] = f1r ? om2 * dlm : 0.0; rs[2] = 0.0; rs[3] = 0.0;
+              rl[0] = 0.0; rl[1] = 0.0; rl[2] = f1r ? odl2b : 0.0; rl[3] = f1r ? odl2b * dlm : 0.0;
+            }
           }
           __pipeline_commit();
         };
@@ -469,7 +486,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           const double* LB = diag ? LA : buf + 3 * SET;
           const int c0 = ci * CH, rows = min(CH, n - c0), rows8 = (rows + 7) & ~7;
           if (tid == 0) n_mma += (unsigned long long)((rows + 3) / 4) * ntile * ntile * 2;
-          if (diag) {   // moments of bin t from the rows of the f1 pixels
+          if (diag && !(NS + 4 <= 64)) {   // moments of bin t from the rows of the f1 pixels
             for (int e = tid; e < 4 * np; e += DT) {
               const int q = e / np, bq = e - q * np;
               const double* src = (q < 2 ? SA : LA) + bq;   // 0: M0, 1: Mi from S; 2: Mj, 3: Mij from L
@@ -482,7 +499,8 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           }
           {
             const int bp0 = 16 * mt + grp, bp1 = bp0 + 8;
-            const bool v0 = bp0 < np, v1 = bp1 < np;
+            const int arows = (diag && NS + 4 <= 64) ? NS + 4 : np;   // A rows NS..NS+3: the moments
+            const bool v0 = bp0 < arows, v1 = bp1 < arows;
             for (int r0 = 0; r0 < rows8; r0 += 8) {
               const int ra = (r0 + kq) * NPAD, rb = ra + 4 * NPAD;
               const double ks0 = kb2[r0 + kq], ks1 = kb2[r0 + kq + 4];
@@ -502,6 +520,23 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             }
           }
           __syncthreads();               // buffer ci & 1 is free for chunk ci + 2
+        }
+        if (diag && NS + 4 <= 64) {   // accumulator rows NS..NS+3: the moments of bin t
+#pragma unroll
+          for (int h2 = 0; h2 < 2; ++h2) {
+            const int q = 16 * mt + grp + 8 * h2 - NS;
+            if (q >= 0 && q < 4) {
+#pragma unroll
+              for (int c = 0; c < CC; ++c) {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                  const int nt8 = ng + nwm * c, bq = 8 * nt8 + 2 * kq + i;
+                  if (nt8 < ntile && bq < np) mom[(q * nt + t) * np + bq] = acc[c][2 * h2 + i];
+                }
+              }
+            }
+          }
+          __syncthreads();
         }
       }
       // flush: column products (subtracted), rank-4 part, diagonal; warp

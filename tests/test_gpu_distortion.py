@@ -35,6 +35,22 @@ def test_distortion_all_pairs_matches_oracle():
     assert np.count_nonzero(Do) > 1000
 
 
+@pytest.mark.parametrize('np_,nt', [(37, 23), (64, 16)])
+def test_distortion_other_binnings(np_, nt):
+    """An odd number of r_par bins (moments from the spare accumulator rows
+    after an odd row length) and 64 r_par bins (no spare rows: the moment loop)."""
+    fs = synthetic.make(3, n=90)
+    am = synthetic.angmax_for(fs)
+    with PairEngine(np_=np_, nt=nt) as eng:
+        eng.upload(fs)
+        eng.build_pairs(am)
+        f1, f2 = eng.get_pairs()
+        D, W = eng.distortion()
+    Do, Wo = O.distortion(fs, f1, f2, np_=np_, nt=nt)
+    _check(D, W, Do, Wo)
+    assert np.count_nonzero(Do) > 1000
+
+
 def test_distortion_edge_catalogue():
     """Length-1 forest (sum w dl^2 = 0), empty and unsorted forests, twins."""
     fs = E.edge_catalog()
