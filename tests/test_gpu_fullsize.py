@@ -44,3 +44,29 @@ def test_config1_fp32_equals_fp64_everywhere():
         ho, co = O.corr(fs, f1[sel], f2[sel], [0, int(sel.sum())])
         assert np.array_equal(c32[s], co[0])
         np.testing.assert_allclose(W32[s], ho[0, O.Q_W], rtol=1e-6, atol=0)
+
+
+def test_config3_distortion_properties():
+    """Whole distortion catalogue (30,000 log-normal forests, all pairs): the
+    oracle cannot restate 1.4e7 forest pairs in a test, so the check is the
+    size-independent one the factored form offers.  W_B of the distortion (the
+    sum of w_i w_j over the pairs of bin B, accumulated from the tensor-core
+    moments) equals the FP64 correlation kernel's W histogram summed over owner
+    pixels, bin for bin, to 1e-12 (the same FP64 bin formula, sums in another
+    order); D is finite and symmetric to 1e-12 of its largest entry (each
+    off-diagonal block is added at (A, B) and (B, A))."""
+    fs = synthetic.make(3)
+    am = synthetic.angmax_for(fs)
+    with PairEngine() as eng:
+        eng.upload(fs)
+        assert eng.build_pairs(am) > 1e7
+        D, WB = eng.distortion()
+        eng.run(kernel=N.KERNEL_FP64_DIAGONAL)
+        h, c = eng.histograms()
+    W = h[:, N.Q_W].sum(axis=0)
+    assert np.array_equal(W != 0, WB != 0)
+    nz = W != 0
+    assert nz.sum() > 2000
+    assert np.max(np.abs(WB[nz] - W[nz]) / np.abs(W[nz])) < 1e-12
+    assert np.all(np.isfinite(D))
+    assert np.abs(D - D.T).max() <= 1e-12 * np.abs(D).max()
