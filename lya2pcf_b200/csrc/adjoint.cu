@@ -78,8 +78,8 @@ __global__ void k_totals(int nslots, int nb, const double* __restrict__ hist, do
 // Reversed-direction flag is in the item index: items [0, n) are (f1, f2),
 // items [n, 2n) are (f2, f1).
 __global__ void __launch_bounds__(256) k_adjoint(const AdjParams p) {
-  extern __shared__ double s_coef[];   // [2][nb]
-  for (int k = threadIdx.x; k < 2 * p.nb; k += blockDim.x) s_coef[k] = p.coef[k];
+  extern __shared__ __align__(16) double s_coef[];   // [nb][2]: g/W, -g xi/W of a bin side by side (one 16-byte load)
+  for (int k = threadIdx.x; k < 2 * p.nb; k += blockDim.x) s_coef[k] = p.coef[(k & 1) * p.nb + (k >> 1)];
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -119,16 +119,40 @@ __global__ void __launch_bounds__(256) k_adjoint(const AdjParams p) {
           while (x < y) { const int m = (x + y) >> 1; if (D2[m] < thi) x = m + 1; else y = m; }
           jhi = x;
         }
-        for (int j = jlo; j < jhi; ++j) {
-          const double d2 = D2[j];
+        // bin of (d1, d2) with the reference FP64 formula, -1 out of range
+        auto pbin = [&](double d2) {
           const double rp = __dmul_rn(fabs(__dsub_rn(d1, d2)), ch);
           const double rt = __dmul_rn(__dadd_rn(d1, d2), sh);
           const double fp = floor(__dmul_rn(rp, p.binner_rp));
           const double ft = floor(__dmul_rn(rt, p.binner_rt));
-          if (fp >= 0.0 && fp < (double)p.np && ft >= 0.0 && ft < (double)p.nt) {
-            const int bin = (int)fp * p.nt + (int)ft;
-            gdw = __fma_rn(s_coef[bin], DW2[j], gdw);
-            gw_ = __fma_rn(s_coef[p.nb + bin], W2[j], gw_);
+          return (fp >= 0.0 && fp < (double)p.np && ft >= 0.0 && ft < (double)p.nt) ? (int)fp * p.nt + (int)ft : -1;
+        };
+        // four partners at a time: independent bin chains, then the sums in partner order
+        int j = jlo;
+        for (; j + 4 <= jhi; j += 4) {
+          int bin[4];
+          double dwj[4], wj[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            bin[u] = pbin(D2[j + u]);
+            dwj[u] = DW2[j + u];
+            wj[u] = W2[j + u];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (bin[u] >= 0) {
+              const double2 cc = reinterpret_cast<const double2*>(s_coef)[bin[u]];
+              gdw = __fma_rn(cc.x, dwj[u], gdw);
+              gw_ = __fma_rn(cc.y, wj[u], gw_);
+            }
+          }
+        }
+        for (; j < jhi; ++j) {
+          const int bn = pbin(D2[j]);
+          if (bn >= 0) {
+            const double2 cc = reinterpret_cast<const double2*>(s_coef)[bn];
+            gdw = __fma_rn(cc.x, DW2[j], gdw);
+            gw_ = __fma_rn(cc.y, W2[j], gw_);
           }
         }
         if (gdw != 0.0) atomicAdd(&p.g_dw[a + i], gdw);

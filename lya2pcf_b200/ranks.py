@@ -1,7 +1,7 @@
 """Ranks of the drop-in drivers: mpi4py when it is installed (as the
 reference, ``2pla.py:13-22``), else ``torch.distributed`` when the process was
-started by torchrun (``WORLD_SIZE`` > 1 in the environment; NCCL when a GPU is
-visible, gloo otherwise), else one process.
+started by torchrun (``WORLD_SIZE`` > 1 in the environment; NCCL when the rank's
+GPU exists, gloo otherwise or when ``LYA2PCF_DIST_BACKEND=gloo``), else one process.
 
 The correlation needs no collective (owner pixels are disjoint; each rank
 writes its own files).  The distortion needs one: :meth:`Ranks.reduce_sum`
@@ -30,9 +30,13 @@ class Ranks:
         if int(os.environ.get('WORLD_SIZE', '1')) > 1:
             import torch
             import torch.distributed as dist
-            self.cuda = torch.cuda.is_available()
+            # NCCL when this rank has a GPU of its own; gloo (host memory) when
+            # LYA2PCF_DIST_BACKEND=gloo asks for it or the rank's GPU does not exist
+            local = int(os.environ.get('LOCAL_RANK', '0'))
+            self.cuda = (os.environ.get('LYA2PCF_DIST_BACKEND', '') != 'gloo' and torch.cuda.is_available()
+                         and local < torch.cuda.device_count())
             if self.cuda:
-                torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
+                torch.cuda.set_device(local)
             dist.init_process_group('nccl' if self.cuda else 'gloo', timeout=datetime.timedelta(seconds=300))
             self.rank, self.size, self.torch_pg = dist.get_rank(), dist.get_world_size(), True
 

@@ -71,8 +71,9 @@ def _reduce_worker(rank, world, port, q):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
-    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
-                      LOCAL_RANK=str(rank))
+    # gloo even where a GPU is visible: the test runs both ranks on one machine
+    os.environ.update(LYA2PCF_DIST_BACKEND='gloo', MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port),
+                      WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank))
     from lya2pcf_b200.ranks import Ranks
     r = Ranks()
     try:
@@ -119,8 +120,9 @@ def _adjoint_worker(rank, world, port, q):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
-    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
-                      LOCAL_RANK=str(rank))
+    # gloo even where a GPU is visible: the test runs both ranks on one machine
+    os.environ.update(LYA2PCF_DIST_BACKEND='gloo', MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port),
+                      WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank))
     from lya2pcf_b200 import synthetic
     from lya2pcf_b200.engine import owner_slots
     from lya2pcf_b200.ranks import Ranks
