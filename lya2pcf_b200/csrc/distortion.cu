@@ -259,7 +259,13 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             nrow = 0;
           }
           if (nrow > 0) {
-            for (int q = lane; q < nrow * np; q += 32) { myS[q] = 0.0; myL[q] = 0.0; }
+            if ((np & 1) == 0) {   // 16-byte stores (both builders start on 16 bytes for even np)
+              double2* s2 = reinterpret_cast<double2*>(myS);
+              double2* l2 = reinterpret_cast<double2*>(myL);
+              for (int q = lane; q < nrow * np / 2; q += 32) { s2[q] = make_double2(0.0, 0.0); l2[q] = make_double2(0.0, 0.0); }
+            } else {
+              for (int q = lane; q < nrow * np; q += 32) { myS[q] = 0.0; myL[q] = 0.0; }
+            }
             __syncwarp();
             const int cnt = jhi - jlo, seg = (cnt + 31) / 32;
             int j = jlo + lane * seg;
@@ -356,10 +362,21 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           double* rs = cS + (size_t)m * TS * NS;
           double* rl = cL + (size_t)m * TS * NS;
           const int off = (lo - wlo) * np;
-          for (int row = 0; row < sp; ++row) {
-            for (int col = lane; col < NS; col += 32) {
-              rs[row * NS + col] = col < np ? myS[off + row * np + col] : 0.0;
-              rl[row * NS + col] = col < np ? myL[off + row * np + col] : 0.0;
+          if ((np & 1) == 0) {   // NS == np: 16-byte copies, every row start on 16 bytes
+            const int h = np / 2;
+            for (int row = 0; row < sp; ++row) {
+              const double2* ss = reinterpret_cast<const double2*>(myS + off + row * np);
+              const double2* sl2 = reinterpret_cast<const double2*>(myL + off + row * np);
+              double2* ds = reinterpret_cast<double2*>(rs + row * NS);
+              double2* dl = reinterpret_cast<double2*>(rl + row * NS);
+              for (int c2 = lane; c2 < h; c2 += 32) { ds[c2] = ss[c2]; dl[c2] = sl2[c2]; }
+            }
+          } else {
+            for (int row = 0; row < sp; ++row) {
+              for (int col = lane; col < NS; col += 32) {
+                rs[row * NS + col] = col < np ? myS[off + row * np + col] : 0.0;
+                rl[row * NS + col] = col < np ? myL[off + row * np + col] : 0.0;
+              }
             }
           }
           if (lane == 0) {
