@@ -160,11 +160,11 @@ def test_adjoint_matches_finite_differences():
             assert abs(fd - grad[p]) <= 1e-5 * max(1.0, abs(fd)), (p, fd, grad[p])
 
 
-def _eta_form_distortion(fs, f1, f2):
+def _eta_form_distortion(fs, f1, f2, np_=50, nt=50):
     """Independent statement of the distortion numerator:
     D_AB = sum_{forest pairs} sum_{(i,j) in A} w_i w_j sum_{(k,l) in B} eta1_ik eta2_jl,
     eta_ik = delta_ik - w_k/Omega - dl_i w_k dl_k / sum(w dl^2)."""
-    nb = 2500
+    nb = np_ * nt
     D = np.zeros((nb, nb))
     WB = np.zeros(nb)
     for a, b in zip(f1, f2):
@@ -173,9 +173,9 @@ def _eta_form_distortion(fs, f1, f2):
         ch, sh = np.sqrt(0.5 * (1 + c)), np.sqrt(0.5 * (1 - c))
         rp = np.abs(A['dc'][:, None] - B['dc'][None, :]) * ch
         rt = (A['dc'][:, None] + B['dc'][None, :]) * sh
-        bp, bt = np.floor(rp * 0.25), np.floor(rt * 0.25)
-        ok = (bp < 50) & (bt < 50)
-        binm = np.where(ok, bp * 50 + bt, -1).astype(int)
+        bp, bt = np.floor(rp * (np_ / 200.0)), np.floor(rt * (nt / 200.0))
+        ok = (bp < np_) & (bt < nt)
+        binm = np.where(ok, bp * nt + bt, -1).astype(int)
 
         def eta(F):
             w, dl = F['w'], F['dl']
@@ -191,7 +191,8 @@ def _eta_form_distortion(fs, f1, f2):
     return D, WB
 
 
-def test_distortion_matches_eta_product_form():
+@pytest.mark.parametrize('np_,nt', [(50, 50), (37, 23), (64, 16)])
+def test_distortion_matches_eta_product_form(np_, nt):
     rng = np.random.default_rng(8)
     import edge_cases as E
     deg = np.pi / 180
@@ -205,8 +206,8 @@ def test_distortion_matches_eta_product_form():
     fs = forestset(F)
     f1 = np.array([0, 0, 1], dtype=np.int32)
     f2 = np.array([1, 2, 2], dtype=np.int32)
-    D, WB = O.distortion(fs, f1, f2)
-    De, WBe = _eta_form_distortion(fs, f1, f2)
+    D, WB = O.distortion(fs, f1, f2, np_=np_, nt=nt)
+    De, WBe = _eta_form_distortion(fs, f1, f2, np_, nt)
     np.testing.assert_allclose(WB, WBe, rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(D, De, rtol=1e-9, atol=1e-9 * np.abs(De).max())
 
