@@ -98,6 +98,7 @@ struct DistParams {
   unsigned long long* next;// [1] work queue counter
   unsigned long long* mma; // [1] block-product work in m8n8k4 units (8x8 tiles, rows rounded to 4), for the roofline
   int shape;               // launch shape (DIST_SHAPES index); part of the captured graph's key
+  int row_offsets;         // 1: the pixel list carries each pixel's scratch row offset (shared memory allows it)
 };
 
 // Bin of a pixel pair with the reference FP64 formula, as (bp, bt); false when
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
   int* tlo = reinterpret_cast<int*>(kbuf + 8 * CH);      // [2][ML]
   int* span = tlo + 2 * ML;                              // [2][ML]
   int* plist = span + 2 * ML;                            // [2*ML] packed (side << 16 | pixel)
+  int* roff = plist + 2 * ML;                            // [2*ML] scratch offset of a listed pixel's row t (row_offsets)
   __shared__ int s_T0, s_T1, s_maxspan, s_cnt;
   __shared__ long long s_item;
 
@@ -428,7 +430,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
           const int Lm = side == 0 ? L1 : L2;
           for (int m = tid; m < Lm; m += DT) {
             const int lo = tlo[side * ML + m], sp = span[side * ML + m];
-            if (sp > 0 && lo <= t && u < lo + sp) plist[atomicAdd(&s_cnt, 1)] = (side << 16) | m;
+            if (sp > 0 && lo <= t && u < lo + sp) {
+              const int x = atomicAdd(&s_cnt, 1);
+              plist[x] = (side << 16) | m;
+              if (p.row_offsets) roff[x] = ((side * ML + m) * TS + t - lo) * NS;   // row u is (u - t) NS further
+            }
           }
         }
         __syncthreads();
@@ -447,11 +453,16 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
             const int sr = (int)__umulhi((unsigned)q, seg_magic), sg = q - sr * segs;
             const int set = sr / CH, r = sr - set * CH;
             if (r >= rows) continue;
-            const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
-            const int lo = tlo[side * ML + m];
             const double* colb = (set & 1) ? colL : colS;
-            const int bin = set < 2 ? t : u;
-            const double* src = colb + (size_t)side * ML * TS * NS + ((size_t)m * TS + (bin - lo)) * NS + 2 * sg;
+            const double* src;
+            if (p.row_offsets) {
+              src = colb + roff[c0 + r] + (set < 2 ? 0 : (u - t) * NS) + 2 * sg;
+            } else {
+              const int pk = plist[c0 + r], side = pk >> 16, m = pk & 0xffff;
+              const int lo = tlo[side * ML + m];
+              const int bin = set < 2 ? t : u;
+              src = colb + (size_t)side * ML * TS * NS + ((size_t)m * TS + (bin - lo)) * NS + 2 * sg;
+            }
             __pipeline_memcpy_async(buf + (size_t)set * SET + (size_t)r * NPAD + 2 * sg, src, 16);
           }
           for (int q = tid; q < nset * (rows8 - rows) * NPAD; q += DT) {
@@ -697,8 +708,13 @@ extern "C" int lya_dist_run(lya_ctx* ctx, double* D, double* W) {
   p.col = ds.col; p.moments = ds.mom; p.D = ds.D; p.W = ds.W; p.err = ds.err; p.next = ds.err + 1;
   p.mma = ds.err + 3;
   p.shape = shape;
-  const size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len + 8 * (size_t)CH) +
-                          sizeof(int) * (6 * (size_t)ds.max_len);
+  size_t smem_run = sizeof(double) * (10 * (size_t)ds.max_len + stage_len + 8 * (size_t)CH) +
+                    sizeof(int) * (6 * (size_t)ds.max_len);
+  // the pixel list's row offsets (one int per listed pixel) when shared memory has room
+  if (smem_run + sizeof(int) * 2 * (size_t)ds.max_len <= 227 * 1024) {
+    smem_run += sizeof(int) * 2 * (size_t)ds.max_len;
+    p.row_offsets = 1;
+  }
   static_assert(sizeof(DistParams) <= sizeof(ds.key), "graph key does not fit");
   cudaError_t e = cudaSuccess;
   if (!ds.graph || memcmp(ds.key, &p, sizeof(p)) != 0) {
