@@ -441,7 +441,11 @@ __global__ void __launch_bounds__(DT, 1) k_dist(const DistParams p) {
         const int n = s_cnt;
         const int nch = (n + CH - 1) / CH;
         // issue the copies of chunk ci into buffer ci & 1 (rows beyond the
-        // chunk are zeroed with plain stores; columns np .. NPAD-1 stay 0)
+        // chunk are zeroed with plain stores).  Columns NS .. NPAD-1 are not
+        // copied: they keep older contents, which reach only accumulator
+        // entries that are never flushed (tile columns >= np), except the
+        // moment columns NS .. NS+3 written below for the A rows of a
+        // diagonal block
         auto issue = [&](int ci) {
           double* buf = stage + (size_t)(ci & 1) * 4 * SET;
           double* kb2 = kbuf + (size_t)(ci & 1) * 4 * CH;
