@@ -17,6 +17,18 @@ import os
 import numpy as np
 
 
+def use_nccl(env=None):
+    """``(nccl, local_rank)`` for a torchrun rank: NCCL when the rank has a GPU
+    of its own (``LOCAL_RANK`` below the visible GPU count); gloo (host memory)
+    when it does not, or when ``LYA2PCF_DIST_BACKEND=gloo`` asks for it."""
+    import torch
+    env = os.environ if env is None else env
+    local = int(env.get('LOCAL_RANK', '0'))
+    nccl = (env.get('LYA2PCF_DIST_BACKEND', '') != 'gloo' and torch.cuda.is_available()
+            and local < torch.cuda.device_count())
+    return nccl, local
+
+
 class Ranks:
     def __init__(self):
         self.comm, self.rank, self.size, self.torch_pg = None, 0, 1, False
@@ -30,11 +42,7 @@ class Ranks:
         if int(os.environ.get('WORLD_SIZE', '1')) > 1:
             import torch
             import torch.distributed as dist
-            # NCCL when this rank has a GPU of its own; gloo (host memory) when
-            # LYA2PCF_DIST_BACKEND=gloo asks for it or the rank's GPU does not exist
-            local = int(os.environ.get('LOCAL_RANK', '0'))
-            self.cuda = (os.environ.get('LYA2PCF_DIST_BACKEND', '') != 'gloo' and torch.cuda.is_available()
-                         and local < torch.cuda.device_count())
+            self.cuda, local = use_nccl()
             if self.cuda:
                 torch.cuda.set_device(local)
             dist.init_process_group('nccl' if self.cuda else 'gloo', timeout=datetime.timedelta(seconds=300))

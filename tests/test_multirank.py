@@ -171,3 +171,17 @@ def test_sharded_adjoint_gradient_reduction():
     mp.start_processes(_adjoint_worker, args=(2, port, q), nprocs=2, join=True, start_method='spawn')
     edw, ew, nshare = q.get(timeout=120)
     assert edw < 1e-12 and ew < 1e-12 and nshare > 0
+
+
+def test_collective_backend_choice(monkeypatch):
+    """NCCL only for a rank whose GPU exists; gloo when asked or when the rank's
+    index is beyond the visible GPUs (two ranks on a one-GPU machine)."""
+    import torch
+    from lya2pcf_b200.ranks import use_nccl
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: True)
+    monkeypatch.setattr(torch.cuda, 'device_count', lambda: 1)
+    assert use_nccl({'LOCAL_RANK': '0'}) == (True, 0)
+    assert use_nccl({'LOCAL_RANK': '1'}) == (False, 1)
+    assert use_nccl({'LOCAL_RANK': '0', 'LYA2PCF_DIST_BACKEND': 'gloo'}) == (False, 0)
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    assert use_nccl({'LOCAL_RANK': '0'}) == (False, 0)
