@@ -676,7 +676,9 @@ __device__ void item_diag2(const CorrParams& p, int64_t t, const SmemHist& h, ty
 // (tables, or the reference FP64 formula inside the guard band).  Sums run over
 // e and s and are scaled to bin units (x = e*cx, y = s*cy) when a run is
 // recorded.  Each lane's first run is classified before the walk, so ragged
-// diagonal starts cost no event; one vote covers two steps (four pairs).
+// diagonal starts cost no event; each step takes one warp vote for events (two
+// pairs per lane), and the loop body holds two steps so the pixel registers
+// rotate without copies.
 // Per-warp state of the forest pair being walked, in shared memory (read on
 // the rare paths only, so the walk's registers hold just the runs, the sums and
 // the pixels); the threshold tables follow it: tlo[np], thi[np], slo[nt], shi[nt].
